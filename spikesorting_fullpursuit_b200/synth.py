@@ -1,0 +1,242 @@
+"""Seeded synthetic recordings for the binary-pursuit workloads.
+
+No public dataset is involved: these recordings stand in for real ones, with
+the shapes and value distributions of the benchmark configurations.
+
+* Noise: white N(0, 1), 4th-order Butterworth band-pass 300-8000 Hz applied
+  forward and backward (``sosfiltfilt``) in float64, rescaled to unit standard
+  deviation per channel, stored as float32.
+* Templates: biphasic differences of Gaussians over the clip window
+  [-1.0, +1.5] ms, trough between -6 and -12 noise sigma at the alignment
+  sample, scaled per channel by a Gaussian fall-off (over channel index, or
+  over probe distance inside a channel neighbourhood; channels outside the
+  neighbourhood are exactly zero).
+* Spike trains: Poisson per unit with a 1.5 ms refractory period; rates uniform
+  or lognormal (median, cap); a fraction of spikes can be moved to within
+  +-1 ms of another unit's spike; each spike's amplitude is scaled by N(1, 0.1).
+* Bias and thresholds follow the noise model of the reference's
+  neuron_separability.compute_separability_metrics + set_bp_threshold
+  (spikesorting_fullpursuit/overlap/neuron_separability.py:113-195, 319-331):
+  theta_t = max(0, -0.5 |T_t|^2 + sigma_bp_noise sqrt(sum_c T_tc' Cov_c T_tc),
+  lower_CI), with the per-channel noise covariance estimated from random clips
+  of the noise-only trace (empirical, zero-mean).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def time_window_to_samples(time_window_s, sampling_rate):
+    """Clip window in samples (spikesorting_fullpursuit/processing/conversions.py:4-39)."""
+    w = list(time_window_s)
+    if w[0] > 0:
+        w[0] *= -1
+    s0 = min(int(round(w[0] * sampling_rate)), 0)
+    s1 = max(int(round(w[1] * sampling_rate)), 1) + 1
+    return [s0, s1], w
+
+
+def band_noise(rng, n_chans, n_samples, fs, lo=300.0, hi=8000.0):
+    from scipy import signal
+    hi = min(hi, 0.45 * fs)
+    sos = signal.butter(4, [lo, hi], btype="band", fs=fs, output="sos")
+    out = np.empty((n_chans, n_samples), dtype=np.float32)
+    for c in range(n_chans):
+        x = rng.standard_normal(n_samples)
+        y = signal.sosfiltfilt(sos, x)
+        y /= np.std(y)
+        out[c] = y.astype(np.float32)
+    return out
+
+
+def channel_positions(layout, n_chans, pitch_um):
+    if layout == "linear":
+        return np.stack([np.zeros(n_chans), np.arange(n_chans) * pitch_um], axis=1)
+    if layout == "two_column":
+        rows = (n_chans + 1) // 2
+        pos = [(col * pitch_um, row * pitch_um) for row in range(rows) for col in range(2)]
+        return np.asarray(pos[:n_chans], dtype=np.float64)
+    return np.stack([np.zeros(n_chans), np.arange(n_chans, dtype=np.float64)], axis=1)
+
+
+def make_templates(rng, n_units, n_chans, fs, clip_width, layout="index", pitch_um=50.0,
+                   nbhd=None, sigma_um=60.0, amp=(6.0, 12.0)):
+    """Templates as an (M, C*W) float32 array, channel-major per template."""
+    win, _ = time_window_to_samples(clip_width, fs)
+    W = win[1] - win[0]
+    t = (np.arange(W) + win[0]) / fs * 1e3  # ms, trough at t = 0
+    pos = channel_positions(layout, n_chans, pitch_um)
+    out = np.zeros((n_units, n_chans, W), dtype=np.float64)
+    for m in range(n_units):
+        s1 = rng.uniform(0.08, 0.16)
+        d = rng.uniform(0.3, 0.5)
+        s2 = rng.uniform(0.2, 0.4)
+        r = rng.uniform(0.2, 0.45)
+        w = -np.exp(-t ** 2 / (2 * s1 ** 2)) + r * np.exp(-(t - d) ** 2 / (2 * s2 ** 2))
+        w = w / -w.min()
+        A = rng.uniform(*amp)
+        if layout == "index":
+            peak = rng.integers(0, n_chans)
+            sig = rng.uniform(0.7, 1.5)
+            g = np.exp(-(np.arange(n_chans) - peak) ** 2 / (2 * sig ** 2))
+        else:
+            lo, hi = pos.min(axis=0), pos.max(axis=0)
+            centre = rng.uniform(lo, hi)
+            dist = np.linalg.norm(pos - centre, axis=1)
+            k = nbhd if np.isscalar(nbhd) else int(rng.integers(nbhd[0], nbhd[1] + 1))
+            keep = np.argsort(dist, kind="stable")[:k]
+            g = np.zeros(n_chans)
+            g[keep] = np.exp(-dist[keep] ** 2 / (2 * sigma_um ** 2))
+            g[keep] /= g[keep].max()
+        out[m] = A * g[:, None] * w[None, :]
+    return out.reshape(n_units, n_chans * W).astype(np.float32), W, -win[0]
+
+
+def spike_trains(rng, n_units, duration_s, fs, rates, refractory_ms=1.5, overlap_frac=0.0,
+                 overlap_ms=1.0):
+    """Spike sample times and unit labels, sorted by time."""
+    refr = refractory_ms * 1e-3
+    times, labels = [], []
+    for m in range(n_units):
+        rate = rates[m]
+        tt = []
+        cur = 0.0
+        mean_isi = max(1.0 / rate - refr, 1e-4)
+        while True:
+            cur += refr + rng.exponential(mean_isi)
+            if cur >= duration_s:
+                break
+            tt.append(cur)
+        times.append(np.asarray(tt))
+        labels.append(np.full(len(tt), m))
+    t_all = np.concatenate(times) if times else np.zeros(0)
+    l_all = np.concatenate(labels) if labels else np.zeros(0, dtype=int)
+    if overlap_frac > 0 and t_all.size > 1 and n_units > 1:
+        n_move = int(round(overlap_frac * t_all.size))
+        movers = rng.choice(t_all.size, size=n_move, replace=False)
+        for i in movers:
+            others = np.flatnonzero(l_all != l_all[i])
+            if others.size == 0:
+                continue
+            j = others[rng.integers(0, others.size)]
+            t_all[i] = t_all[j] + rng.uniform(-overlap_ms, overlap_ms) * 1e-3
+        # restore each unit's refractory period after the moves
+        keep = np.ones(t_all.size, dtype=bool)
+        for m in range(n_units):
+            idx = np.flatnonzero(l_all == m)
+            order = idx[np.argsort(t_all[idx], kind="stable")]
+            last = -np.inf
+            for k in order:
+                if t_all[k] - last < refr:
+                    keep[k] = False
+                else:
+                    last = t_all[k]
+        t_all, l_all = t_all[keep], l_all[keep]
+    samples = np.round(t_all * fs).astype(np.int64)
+    order = np.argsort(samples, kind="stable")
+    return samples[order], l_all[order].astype(np.int64)
+
+
+def noise_covariance(rng, noise, W, n_clips=10000):
+    C, N = noise.shape
+    n_clips = int(min(n_clips, max(1, N - W - 1)))
+    starts = rng.integers(0, N - W, size=n_clips)
+    idx = starts[:, None] + np.arange(W)[None, :]
+    covs = []
+    for c in range(C):
+        X = noise[c][idx].astype(np.float64)
+        covs.append(X.T @ X / n_clips)
+    return covs
+
+
+def separability_metrics(templates, covs, n_chans, W, sigma_bp_noise=3.719, sigma_bp_CI=None):
+    """Bias/threshold inputs of binary_pursuit (neuron_separability.py:113-195, 319-331)."""
+    T = np.asarray(templates, dtype=np.float64)
+    M = T.shape[0]
+    ci = np.inf if sigma_bp_CI is None else sigma_bp_CI
+    ss = np.sum(T ** 2, axis=1)
+    var = np.zeros(M)
+    for n in range(M):
+        for c in range(n_chans):
+            tc = T[n, c * W:(c + 1) * W]
+            var[n] += tc @ covs[c] @ tc
+    lower_ci = 0.5 * ss - ci * np.sqrt(var)
+    thr = -0.5 * ss + sigma_bp_noise * np.sqrt(var)
+    thr = np.maximum(np.maximum(thr, 0.0), lower_ci)
+    return {
+        "bp_n_samples_per_chan": W,
+        "templates": np.asarray(templates),
+        "template_SS": ss,
+        "template_SS_by_chan": np.zeros((M, n_chans)),
+        "neuron_variances": var,
+        "neuron_lower_thresholds": thr,
+        "neuron_lower_CI": lower_ci,
+    }
+
+
+def make_recording(seed, n_chans=4, fs=40000, duration_s=1.0, n_units=6, layout="index",
+                   pitch_um=50.0, nbhd=None, sigma_um=60.0, rate_model=("uniform", 5.0, 30.0),
+                   overlap_frac=0.0, clip_width=(-1.0e-3, 1.5e-3), amp=(6.0, 12.0),
+                   add_spikes=True, n_cov_clips=10000):
+    """A full binary_pursuit input set: voltage, sort_info, separability_metrics."""
+    rng = np.random.default_rng(seed)
+    n_samples = int(round(duration_s * fs))
+    clip_width = list(clip_width)
+    templates, W, pre = make_templates(rng, n_units, n_chans, fs, clip_width, layout, pitch_um,
+                                       nbhd, sigma_um, amp)
+    if rate_model[0] == "uniform":
+        rates = rng.uniform(rate_model[1], rate_model[2], size=n_units)
+    else:
+        rates = np.minimum(np.exp(rng.normal(np.log(rate_model[1]), 0.6, size=n_units)),
+                           rate_model[2])
+    noise = band_noise(rng, n_chans, n_samples, fs)
+    covs = noise_covariance(rng, noise, W, n_cov_clips)
+    voltage = noise.copy()
+    times, labels = spike_trains(rng, n_units, duration_s, fs, rates, overlap_frac=overlap_frac)
+    scales = rng.normal(1.0, 0.1, size=times.size)
+    if add_spikes and times.size:
+        onset = times - pre
+        ok = (onset >= 0) & (onset + W <= n_samples)
+        onset, lab, sc = onset[ok], labels[ok], scales[ok]
+        T3 = templates.reshape(n_units, n_chans, W)
+        cols = onset[:, None] + np.arange(W)[None, :]
+        for c in range(n_chans):
+            vals = sc[:, None] * T3[lab, c, :]
+            if not np.any(vals):
+                continue
+            np.add.at(voltage[c], cols.ravel(), vals.ravel().astype(np.float32))
+    sort_info = {
+        "sampling_rate": fs,
+        "clip_width": clip_width,
+        "n_samples_per_chan": W,
+        "n_channels": n_chans,
+        "n_samples": n_samples,
+        "do_overlap_recheck": True,
+        "get_adjusted_clips": False,
+        "sigma_bp_noise": 3.719,
+        "sigma_bp_CI": None,
+    }
+    metrics = separability_metrics(templates, covs, n_chans, W)
+    truth = {"times": times, "labels": labels, "scales": scales}
+    return voltage, sort_info, metrics, truth
+
+
+# Shapes of the benchmark configurations (durations in seconds).
+CONFIGS = {
+    "tetrode": dict(n_chans=4, fs=40000, duration_s=30.0, n_units=6, layout="index",
+                    rate_model=("uniform", 5.0, 30.0)),
+    "linear16": dict(n_chans=16, fs=40000, duration_s=600.0, n_units=40, layout="linear",
+                     pitch_um=50.0, nbhd=(4, 6), sigma_um=60.0,
+                     rate_model=("lognormal", 10.0, 80.0), overlap_frac=0.2),
+    "dense64": dict(n_chans=64, fs=30000, duration_s=1800.0, n_units=200, layout="two_column",
+                    pitch_um=25.0, nbhd=8, sigma_um=40.0,
+                    rate_model=("lognormal", 8.0, 100.0), overlap_frac=0.25),
+}
+
+
+def config_recording(name, seed, duration_s=None, **overrides):
+    kw = dict(CONFIGS[name])
+    if duration_s is not None:
+        kw["duration_s"] = duration_s
+    kw.update(overrides)
+    return make_recording(seed, **kw)
