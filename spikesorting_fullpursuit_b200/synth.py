@@ -139,6 +139,8 @@ def spike_trains(rng, n_units, duration_s, fs, rates, refractory_ms=1.5, overlap
 
 def noise_covariance(rng, noise, W, n_clips=10000):
     C, N = noise.shape
+    if N <= W + 1:  # too short to sample a clip: unit-variance white noise
+        return [np.eye(W) for _ in range(C)]
     n_clips = int(min(n_clips, max(1, N - W - 1)))
     starts = rng.integers(0, N - W, size=n_clips)
     idx = starts[:, None] + np.arange(W)[None, :]
@@ -151,10 +153,11 @@ def noise_covariance(rng, noise, W, n_clips=10000):
 
 def separability_metrics(templates, covs, n_chans, W, sigma_bp_noise=3.719, sigma_bp_CI=None):
     """Bias/threshold inputs of binary_pursuit (neuron_separability.py:113-195, 319-331)."""
-    T = np.asarray(templates, dtype=np.float64)
+    T = np.asarray(templates)
     M = T.shape[0]
     ci = np.inf if sigma_bp_CI is None else sigma_bp_CI
-    ss = np.sum(T ** 2, axis=1)
+    # summed in the templates' own dtype, as neuron_separability.py:132-134 does
+    ss = np.sum(T ** 2, axis=1).astype(np.float64)
     var = np.zeros(M)
     for n in range(M):
         for c in range(n_chans):
