@@ -1,0 +1,353 @@
+"""Benchmark: binary-pursuit throughput (Msample*ch/s) on B200.
+
+Workload (default): the 16-channel linear-probe recording, 40 kHz, 10 min
+float32 (N = 24e6 samples per channel), 40 templates of 101 samples/channel on
+4-6 channel neighbourhoods, lognormal rates (median 10 Hz, cap 80 Hz), 20% of
+spikes forced to overlap, overlap recheck on with n_max_shift_inds = W - 1.
+Synthetic, seeded (spikesorting_fullpursuit_b200.synth); no dataset.
+
+A step is one full binary pursuit of the recording (all passes, overlap
+recheck included) -- the unit the metric is quoted on.
+* value: device-resident throughput of the chosen ("fast") path: the chunk's
+  voltage is already in HBM; per step the pristine voltage is restored into
+  the working buffer outside the timed interval; each step is timed with CUDA
+  events on the launching stream; inputs (1.5 GB voltage, 3.8 GB likelihood)
+  are far larger than L2.
+* e2e: the public API binary_pursuit() with host numpy voltage in and host
+  numpy spikes out (host<->device copies inside the timed region).
+* plain_fp32: the plain FP32 path on the same data, and the fraction of spikes
+  (index, label) the chosen path shares with it.
+
+Multi-GPU (torchrun): the path shards by recording (each rank pursues its own
+recording, no data-path collective): weak scaling, max time over ranks.
+
+--impl reference: the reference's OpenCL kernels compiled for the host CPU
+(oracle/_ref) on a bounded leading slice of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import copy
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "binary-pursuit Msample·ch/s, chosen vs plain FP32 on B200, ≥99.9% spike match"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="linear16", choices=["linear16", "tetrode", "dense64"])
+    p.add_argument("--duration", type=float, default=None, help="seconds of recording (default: config's)")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-s", type=float, default=2.0)
+    return p.parse_args()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def run_reference(args, rank):
+    """The reference kernels on the host cores, bounded slice of the workload."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    from spikesorting_fullpursuit_b200 import synth
+    import ref_host
+    sample_s = args.cpu_sample_s
+    V, si, sm, _ = synth.config_recording(args.config, seed=1, duration_s=sample_s)
+    W = si["n_samples_per_chan"]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ref_host.binary_pursuit(V, si, copy.deepcopy(sm), n_max_shift_inds=W - 1)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    tot = float(np.sum(times))
+    value = V.shape[0] * V.shape[1] * len(times) / tot / 1e6
+    cores = ref_host.threads()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Msample*ch/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "%s (leading %.1f s slice)" % (args.config, sample_s)},
+        "cpu_baseline": {"value": value, "unit": "Msample*ch/s", "cores": cores, "kind": "reference",
+                         "sample": "leading %.1f s of the %s recording, %d channels, reference OpenCL "
+                                   "kernels compiled for the CPU, host loop restated" %
+                                   (sample_s, args.config, V.shape[0])},
+        "e2e": {"value": value, "unit": "Msample*ch/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    from spikesorting_fullpursuit_b200 import _native, binary_pursuit, synth
+    from spikesorting_fullpursuit_b200.overlap.binary_pursuit_parallel import plan_chunks
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=dev)
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+    V, si, sm, truth = synth.config_recording(args.config, seed=1 + rank, duration_s=args.duration)
+    C, N = V.shape
+    W = si["n_samples_per_chan"]
+    S = W - 1
+    T = np.float32(sm["templates"])
+    M = T.shape[0]
+    bias = np.float32(-0.5 * sm["template_SS"])
+    theta = np.float32(sm["neuron_lower_thresholds"])
+    total_mem = torch.cuda.get_device_properties(dev).total_memory
+    onsets, chunk = plan_chunks(N, C, M, W, si["sampling_rate"], S, total_mem)
+    assert len(onsets) == 1 and chunk >= N, "workload must fit one chunk"
+    lib = _native.lib()
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    Vd0 = torch.from_numpy(V).to(dev)
+    Vw = torch.empty_like(Vd0)
+    Td = torch.from_numpy(T).to(dev)
+    bd = torch.from_numpy(bias).to(dev)
+    thd = torch.from_numpy(theta).to(dev)
+    d = _native.dims(C, N, M, W, S)
+    cap = 4 * (N // W + 1) + 1024
+    idx = torch.empty(cap, dtype=torch.int32, device=dev)
+    lab = torch.empty(cap, dtype=torch.int32, device=dev)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def run_mode(mode_flags, steps, warmup, timing=False):
+        flags = mode_flags | _native.FBP_OVERLAP_RECHECK | (_native.FBP_TIMING if timing else 0)
+        ws = torch.empty(_native.workspace_bytes(d, flags), dtype=torch.uint8, device=dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms, stats, result = [], None, None
+        for i in range(warmup + steps):
+            Vw.copy_(Vd0)
+            n = ctypes.c_uint32(0)
+            st = _native.FbpChunkStats()
+            if i == warmup:
+                if world > 1:
+                    dist.barrier()
+                torch.cuda.synchronize()
+            ev0.record(stream)
+            _native.check(lib.fbp_pursue_chunk(ctypes.byref(d), flags, P(Vw), P(Td), P(bd), P(thd), P(ws),
+                                               ws.numel(), P(idx), P(lab), cap, ctypes.byref(n),
+                                               ctypes.byref(st), 0, sptr))
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            if i >= warmup:
+                ms.append(ev0.elapsed_time(ev1))
+            stats = st.as_dict()
+            k = n.value
+            result = (idx[:k].cpu().numpy(), lab[:k].cpu().numpy())
+        del ws
+        return ms, stats, result
+
+    # chosen path, device-resident
+    with Clocks(local) as clk:
+        ms_fast, st_fast, res_fast = run_mode(0, args.steps, args.warmup)
+    clocks = clk.summary()
+    t_fast = sum(ms_fast)
+    if world > 1:
+        t = torch.tensor([t_fast], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_fast = float(t.item())
+    units = C * N * args.steps * world
+    value = units / (t_fast * 1e-3) / 1e6
+    # per-stage breakdown (separate untimed run with stage events)
+    _, st_stage, _ = run_mode(0, 1, 0, timing=True)
+
+    # e2e through the public API (host in, host out)
+    sm_e2e = copy.deepcopy(sm)
+    binary_pursuit(V, np.float32, si, sm_e2e, n_max_shift_inds=S, verbose=False)  # warm
+    e2e_ms = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = binary_pursuit(V, np.float32, si, copy.deepcopy(sm), n_max_shift_inds=S, verbose=False)
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_t = float(np.sum(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_t], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e_value = C * N * len(e2e_ms) * world / (e2e_t * 1e-3) / 1e6
+    n_sp = len(out[0])
+
+    plain = None
+    if not args.no_plain:
+        ms_plain, st_plain, res_plain = run_mode(_native.FBP_PLAIN_FP32, 1, 1)
+        a = set(zip(res_fast[0].tolist(), res_fast[1].tolist()))
+        b = set(zip(res_plain[0].tolist(), res_plain[1].tolist()))
+        match = len(a & b) / max(1, len(a | b))
+        plain = {"value": C * N / (ms_plain[0] * 1e-3) / 1e6, "unit": "Msample*ch/s",
+                 "ms_per_step": ms_plain[0], "spike_match": match,
+                 "identical_order": bool(np.array_equal(res_fast[0], res_plain[0])
+                                         and np.array_equal(res_fast[1], res_plain[1])),
+                 "stages_ms": {k: v for k, v in st_plain.items() if k.startswith("ms_")}}
+
+    hbm, tflops, peak_kind = load_peaks()
+    # dominant stage and its roofline
+    stages = {k[3:]: v for k, v in st_stage.items() if k.startswith("ms_") and k != "ms_total"}
+    dom = max(stages, key=stages.get)
+    listed = st_stage["listed"]
+    lik_flop = 2.0 * M * C * W * W * listed
+    if dom == "likelihood":
+        achieved = lik_flop / (stages[dom] * 1e-3) / 1e12
+        roof = {"kernel": "likelihood", "bound": "tensor", "achieved": achieved, "peak": tflops,
+                "unit": "TFLOP/s", "frac": achieved / tflops, "traffic": None,
+                "peak_kind": peak_kind}
+    elif dom == "overlap":
+        flagged = st_stage["flagged"]
+        flop = 2.0 * C * W * M * (2 * S + 1) * flagged
+        achieved = flop / (stages[dom] * 1e-3) / 1e12
+        roof = {"kernel": "overlap_recheck", "bound": "tensor", "achieved": achieved, "peak": tflops,
+                "unit": "TFLOP/s", "frac": achieved / tflops, "traffic": None, "peak_kind": peak_kind}
+    else:
+        byts = 4.0 * M * N * 3 + 12.0 * N / W
+        achieved = byts / (stages[dom] * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Msample*ch/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fast / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "%s: %d ch x %d samples (%.0f s at %d Hz), %d templates x %d samples, "
+                                   "S=%d, overlap recheck on" % (args.config, C, N, N / si["sampling_rate"],
+                                                                si["sampling_rate"], M, W, S),
+                       "l2": "inputs larger than L2 (voltage %.2f GB, likelihood %.2f GB)" % (
+                           4 * C * N / 1e9, 4 * M * N / 1e9),
+                       "spikes": n_sp, "passes": st_fast["passes"], "mode": "fast"},
+            "e2e": {"value": e2e_value, "unit": "Msample*ch/s", "h2d_bytes_per_step": int(4 * C * N + T.nbytes + 8 * M),
+                    "d2h_bytes_per_step": int(8 * n_sp), "ms_per_step": e2e_t / len(e2e_ms)},
+            "gpu_launches": None,
+            "stages_ms": stages,
+            "stats": {k: st_stage[k] for k in ("passes", "n_spikes", "listed", "flagged", "fixups", "pair_exact")},
+            "roofline": roof,
+            "plain_fp32": plain,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(args):
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    from spikesorting_fullpursuit_b200 import synth
+    sample_s = args.cpu_sample_s
+    V, si, sm, _ = synth.config_recording(args.config, seed=1, duration_s=sample_s)
+    W = si["n_samples_per_chan"]
+    try:
+        import ref_host
+        kind = "reference"
+        t0 = time.perf_counter()
+        ref_host.binary_pursuit(V, si, copy.deepcopy(sm), n_max_shift_inds=W - 1)
+        dt = time.perf_counter() - t0
+        cores = ref_host.threads()
+        what = "reference OpenCL kernels compiled for the CPU (oracle/_ref), host loop restated"
+    except Exception:  # reference library not built: the oracle port
+        import oracle as _oracle
+        kind = "port"
+        t0 = time.perf_counter()
+        _oracle.binary_pursuit(V, np.float32, si, copy.deepcopy(sm), n_max_shift_inds=W - 1)
+        dt = time.perf_counter() - t0
+        cores = os.cpu_count()
+        what = "C restatement (oracle) with OpenMP"
+    return {"value": V.shape[0] * V.shape[1] / dt / 1e6, "unit": "Msample*ch/s", "cores": cores,
+            "kind": kind, "sample": "leading %.1f s of the %s recording (%d ch); %s" % (
+                sample_s, args.config, V.shape[0], what)}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,132 @@
+/*
+ * fbp.h -- C ABI of libfbp.so, the B200 (sm_100a) binary-pursuit library.
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA global-memory
+ * addresses on the current device; `stream` is a cudaStream_t passed as void*
+ * (NULL = legacy default stream).  No call allocates device memory: the caller
+ * owns every buffer, including the workspace sized by fbp_workspace_bytes().
+ * Every call returns an fbp_status; the text of the last error of the calling
+ * thread is available from fbp_last_error().
+ *
+ * Layouts (identical to the reference kernels,
+ * spikesorting_fullpursuit/kernels/binary_pursuit.cl:11-29):
+ *   voltage    float32 [C][N]     channel-major, N samples per channel
+ *   templates  float32 [M][C][W]  W samples per channel, channel-major per template
+ *   likelihood float32 [M][N]
+ */
+#ifndef FBP_H
+#define FBP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FBP_ABI_VERSION 1
+
+typedef enum fbp_status {
+    FBP_OK = 0,
+    FBP_E_ARG = -1,        /* bad shape, null pointer or size */
+    FBP_E_WORKSPACE = -2,  /* workspace smaller than fbp_workspace_bytes() */
+    FBP_E_CAPACITY = -3,   /* more spikes than the output capacity */
+    FBP_E_PASSES = -4,     /* pass limit reached before convergence */
+    FBP_E_CUDA = -5,       /* a CUDA call failed; see fbp_last_error() */
+    FBP_E_DEVICE = -6      /* a kernel reported an error status word */
+} fbp_status;
+
+/* Option bits of fbp_pursue_chunk. */
+#define FBP_OVERLAP_RECHECK 0x1u  /* sort_info["do_overlap_recheck"] */
+#define FBP_PLAIN_FP32      0x2u  /* plain FP32 kernels: scalar likelihood, brute-force recheck */
+
+/* Sizes of one chunk of the pursuit. */
+typedef struct fbp_dims {
+    uint32_t n_chans;      /* C */
+    uint32_t n_samples;    /* N, samples per channel in the chunk (> W) */
+    uint32_t n_templates;  /* M */
+    uint32_t template_len; /* W, samples per channel of a template (window length) */
+    uint32_t n_max_shift;  /* S, n_max_shift_inds of the overlap recheck */
+    uint32_t work_group;   /* work-group size whose order the results follow (power of two, 256) */
+} fbp_dims;
+
+/* Counters of one fbp_pursue_chunk call. */
+typedef struct fbp_chunk_stats {
+    int32_t passes;          /* pursuit passes run (the last one adds no spike) */
+    uint32_t n_spikes;       /* spikes written */
+    uint64_t listed;         /* windows whose likelihood was (re)computed, summed over passes */
+    uint64_t flagged;        /* windows given to the overlap recheck, summed over passes */
+    uint64_t fixups;         /* likelihood samples recomputed exactly after the tensor-core pass */
+    uint64_t pair_exact;     /* overlap items whose pair likelihood was computed exactly */
+    float ms_likelihood;     /* device time per stage, summed over passes (0 unless timing) */
+    float ms_argmax;
+    float ms_overlap;
+    float ms_accept;
+    float ms_residual;
+    float ms_total;
+} fbp_chunk_stats;
+
+/* Library ABI version (FBP_ABI_VERSION). */
+int fbp_abi_version(void);
+
+/* Text of the last error on the calling thread ("" if none). */
+const char* fbp_last_error(void);
+
+/* Bytes of device workspace fbp_pursue_chunk needs for these sizes and flags.
+ * Returns 0 for invalid sizes. */
+size_t fbp_workspace_bytes(const fbp_dims* dims, uint32_t flags);
+
+/* One chunk of binary pursuit: the loop of
+ * spikesorting_fullpursuit/overlap/binary_pursuit_parallel.py:907-1356 with the
+ * kernels compute_full_likelihood, compute_template_maximum_likelihood,
+ * overlap_recheck_indices, parse_overlap_recheck_indices,
+ * check_overlap_reassignments, binary_pursuit and compute_residual
+ * (binary_pursuit.cl:57-1063), run on the device until a pass adds no spike.
+ *   voltage   in: the chunk's voltage; out: the residual (spikes subtracted)
+ *   bias      float32[M], -0.5*template_SS (binary_pursuit_parallel.py:258)
+ *   theta     float32[M], neuron_lower_thresholds (binary_pursuit_parallel.py:262)
+ *   spike_idx, spike_lab  uint32[capacity]: spike onsets (chunk-relative) and
+ *             template rows, pass by pass, each pass in window order
+ *   n_spikes  host out: number of spikes written
+ *   stats     host out, may be NULL
+ *   max_passes  0 = no limit
+ * The call synchronises with `stream` once per pass to read the pass's spike
+ * count. */
+int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* voltage,
+                     const float* templates, const float* bias, const float* theta,
+                     void* workspace, size_t workspace_bytes,
+                     uint32_t* spike_idx, uint32_t* spike_lab, uint32_t capacity,
+                     uint32_t* n_spikes, fbp_chunk_stats* stats, int32_t max_passes,
+                     void* stream);
+
+/* Adjusted clips: clips[k][c][j] = residual[c][idx_k + j] + templates[lab_k][c][j]
+ * for idx_k + j < N, else left untouched (get_adjusted_clips,
+ * binary_pursuit.cl:1088-1130).  clips is float32 [n][C*W]. */
+int fbp_adjusted_clips(const fbp_dims* dims, const float* residual, const float* templates,
+                       const uint32_t* spike_idx, const uint32_t* spike_lab, uint32_t n,
+                       float* clips, void* stream);
+
+/* Likelihood of the listed windows (compute_full_likelihood,
+ * binary_pursuit.cl:255-300): L[t][s] = bias[t] + sum_c sum_j T[t][c][j] V[c][s+j]
+ * for s in [w*W, min((w+1)*W, N)), 0 where s+W >= N.  windows = NULL means all
+ * ceil(N/W) windows.  mode 0: plain FP32 kernel; mode 1: tensor-core estimate
+ * with exact FP32 recomputation of every sample that can be positive.  Both
+ * give the reference's float32 result wherever it is > 0 and a value <= 0
+ * wherever it is <= 0 (mode 0 is bit-exact everywhere).  workspace: as for
+ * fbp_pursue_chunk (same dims, flags 0). */
+int fbp_likelihood(const fbp_dims* dims, int mode, const float* voltage, const float* templates,
+                   const float* bias, const uint32_t* windows, uint32_t n_windows, float* likelihood,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Residual subtraction of n spikes in order (compute_residual,
+ * binary_pursuit.cl:57-102): voltage[c][idx_k + j] -= templates[lab_k][c][j].
+ * Spikes whose ranges overlap are applied in list order. */
+int fbp_residual(const fbp_dims* dims, float* voltage, const float* templates,
+                 const uint32_t* spike_idx, const uint32_t* spike_lab, uint32_t n,
+                 void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FBP_H */

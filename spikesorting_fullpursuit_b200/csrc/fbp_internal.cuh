@@ -1,0 +1,133 @@
+// fbp_internal.cuh -- shared definitions of libfbp.so (B200, sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstddef>
+#include <string>
+
+#include "../../include/fbp.h"
+
+namespace fbp {
+
+// ---------------------------------------------------------------------------
+// Error reporting
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+
+#define FBP_CUDA(expr)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (expr);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return ::fbp::fail(FBP_E_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device status word: counters the kernels of one pass publish.
+// ---------------------------------------------------------------------------
+struct DevStatus {
+    uint32_t n_flag;        // windows flagged for the overlap recheck this pass
+    uint32_t n_spikes;      // spikes accepted this pass
+    uint32_t n_next;        // windows listed for the next pass
+    uint32_t chain_overflow;// a prune/reassign chain was longer than the walk limit
+    uint32_t error;         // nonzero: a kernel detected an inconsistent state
+    uint32_t n_fix;         // likelihood samples queued for exact recomputation
+    uint32_t n_pair_exact;  // overlap items recomputed exactly
+    uint32_t n_conf;        // spikes of this pass overlapping an earlier one
+    unsigned long long pair_items;  // items evaluated by the overlap recheck
+};
+
+// ---------------------------------------------------------------------------
+// Workspace layout (all offsets 256-byte aligned)
+// ---------------------------------------------------------------------------
+struct Layout {
+    uint64_t C, N, M, W, S, WG, nw, nwf, nblk;
+    size_t off_L, off_best_lik, off_best_lab, off_best_idx, off_ov_idx, off_ov_lab;
+    size_t off_check, off_orech, off_orech_fin, off_list, off_list2, off_flag;
+    size_t off_has, off_newval, off_pidx, off_plab, off_pwin, off_pconf, off_keys;
+    size_t off_blk, off_status;
+    // tensor-core likelihood (mode 1)
+    size_t off_vt_hi, off_vt_lo, off_tt_hi, off_tt_lo, off_fix, off_tnorm;
+    uint64_t Cp, Kt, Mp, n_fix_cap;
+    size_t bytes;
+};
+
+bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L);
+
+struct Work {
+    const Layout* lay;
+    unsigned char* base;
+    template <class T>
+    T* at(size_t off) const { return reinterpret_cast<T*>(base + off); }
+    float* L() const { return at<float>(lay->off_L); }
+    float* best_lik() const { return at<float>(lay->off_best_lik); }
+    uint32_t* best_lab() const { return at<uint32_t>(lay->off_best_lab); }
+    uint32_t* best_idx() const { return at<uint32_t>(lay->off_best_idx); }
+    uint32_t* ov_idx() const { return at<uint32_t>(lay->off_ov_idx); }
+    uint32_t* ov_lab() const { return at<uint32_t>(lay->off_ov_lab); }
+    uint8_t* check() const { return at<uint8_t>(lay->off_check); }
+    uint8_t* orech() const { return at<uint8_t>(lay->off_orech); }
+    uint8_t* orech_fin() const { return at<uint8_t>(lay->off_orech_fin); }
+    uint32_t* list() const { return at<uint32_t>(lay->off_list); }
+    uint32_t* list2() const { return at<uint32_t>(lay->off_list2); }
+    uint32_t* flag() const { return at<uint32_t>(lay->off_flag); }
+    uint8_t* has() const { return at<uint8_t>(lay->off_has); }
+    uint8_t* newval() const { return at<uint8_t>(lay->off_newval); }
+    uint32_t* pidx() const { return at<uint32_t>(lay->off_pidx); }
+    uint32_t* plab() const { return at<uint32_t>(lay->off_plab); }
+    uint32_t* pwin() const { return at<uint32_t>(lay->off_pwin); }
+    uint8_t* pconf() const { return at<uint8_t>(lay->off_pconf); }
+    unsigned long long* keys() const { return at<unsigned long long>(lay->off_keys); }
+    uint32_t* blk() const { return at<uint32_t>(lay->off_blk); }
+    DevStatus* status() const { return at<DevStatus>(lay->off_status); }
+};
+
+// Sizes passed by value to kernels.
+struct Dims {
+    uint32_t C, N, M, W, S, WG, nw, nwf;
+};
+
+inline Dims dims_of(const Layout& l)
+{
+    return Dims{(uint32_t)l.C, (uint32_t)l.N, (uint32_t)l.M, (uint32_t)l.W,
+                (uint32_t)l.S, (uint32_t)l.WG, (uint32_t)l.nw, (uint32_t)l.nwf};
+}
+
+// ---------------------------------------------------------------------------
+// Launchers (kernels_plain.cu)
+// ---------------------------------------------------------------------------
+int launch_iota(uint32_t* list, uint32_t n, cudaStream_t st);
+int launch_likelihood_exact(const Dims& d, const float* V, const float* T, const float* bias,
+                            const uint32_t* list, uint32_t nlist, float* L, cudaStream_t st);
+int launch_argmax(const Dims& d, const Work& w, const uint32_t* list, uint32_t nlist,
+                  cudaStream_t st);
+int launch_compact_flagged(const Dims& d, const Work& w, uint32_t nlist, cudaStream_t st);
+int launch_overlap_plain(const Dims& d, const Work& w, const float* V, const float* T,
+                         const float* theta, uint32_t nflag_max, cudaStream_t st);
+int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint32_t nflag_max,
+                          cudaStream_t st);
+int launch_accept(const Dims& d, const Work& w, const float* theta, uint32_t nlist,
+                  cudaStream_t st);
+int launch_next_list(const Dims& d, const Work& w, cudaStream_t st);
+int launch_residual(const Dims& d, const Work& w, float* V, const float* T,
+                    const uint32_t* idx, const uint32_t* lab, const uint32_t* win, uint32_t n,
+                    cudaStream_t st);
+int launch_adjusted_clips(const Dims& d, const float* V, const float* T, const uint32_t* idx,
+                          const uint32_t* lab, uint32_t n, float* clips, cudaStream_t st);
+
+// Tensor-core likelihood (lik_tc.cu)
+bool tc_supported(const Dims& d);
+int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T,
+                         const float* bias, const uint32_t* list, uint32_t nlist, float* L,
+                         bool refresh_voltage, cudaStream_t st, uint64_t* n_fix_out);
+int launch_tc_prepare_templates(const Dims& d, const Work& w, const float* T, cudaStream_t st);
+int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const uint32_t* idx,
+                             const uint32_t* win, uint32_t n, bool all, cudaStream_t st);
+
+// Screened overlap recheck (overlap_fast.cu)
+int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const float* T,
+                        const float* theta, uint32_t nflag_max, cudaStream_t st);
+
+}  // namespace fbp

@@ -1,0 +1,215 @@
+"""Drop-in binary_pursuit() on a B200.
+
+Same signature, arguments, return values and side effect as
+spikesorting_fullpursuit.overlap.binary_pursuit_parallel.binary_pursuit
+(binary_pursuit_parallel.py:175-1532):
+
+    binary_pursuit(voltage, v_dtype, sort_info, separability_metrics,
+                   n_max_shift_inds=None, kernels_path=None, max_gpu_memory=None)
+      -> (event_indices int64[n], neuron_labels int64[n],
+          binary_pursuit_spike_bool bool[n], adjusted_clips)
+
+The pursuit of each chunk runs in libfbp.so (hand-written sm_100a CUDA behind
+the C ABI of include/fbp.h) on PyTorch-owned device buffers.  Chunking follows
+the reference's device-memory planner with this GPU's memory, so chunk
+boundaries (and the duplicate spikes the reference leaves in the 3W chunk
+overlaps) are the reference's.  Results equal the reference kernels run with
+their work-groups in order (see include/fbp.h and DESIGN.md).
+
+Differences, all documented:
+* ``kernels_path`` is accepted and ignored (there is no OpenCL source).
+* If the first pass of a chunk flags no window for the overlap recheck the
+  reference raises UnboundLocalError (binary_pursuit_parallel.py:1369-1371
+  releases buffers it never created); this implementation returns the empty
+  result it was meant to return.
+* Keyword-only extras: ``mode`` ("fast": tensor-core likelihood and screened
+  overlap recheck, both exact; "plain": scalar FP32 kernels), ``device``,
+  ``work_group_size`` (the reference's kernel work-group size, 256, whose
+  execution order the results follow), ``verbose``, ``return_stats``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .. import _native
+from ..processing.conversions import time_window_to_samples
+
+WORK_GROUP_SIZE = 256
+
+
+def plan_chunks(n_samples, n_chans, n_templates, template_samples_per_chan, sampling_rate,
+                n_max_shift_inds, global_mem_size, max_gpu_memory=None,
+                work_group_size=WORK_GROUP_SIZE, address_bits=64):
+    """Chunk onsets and chunk length from the device-memory budget.
+
+    Follows binary_pursuit_parallel.py:389-475 (budget per second of data:
+    voltage, likelihood, per-window buffers and the overlap group buffers) and
+    :498-507 (onsets overlap by 3 windows).  Arithmetic types follow the
+    reference so the floor() lands on the same sample count."""
+    W = int(template_samples_per_chan)
+    budget = max(global_mem_size * 0.5, global_mem_size - (1024 * 1024 * 1024))
+    if max_gpu_memory is not None:
+        budget = min(budget, max_gpu_memory)
+    assert budget > 0
+    S = int(n_max_shift_inds)
+    items = np.int64((2 * S + 1) * (2 * S + 1) * n_templates)
+    groups = np.int64(((items - 1) / np.int64(work_group_size)) + 1)
+    fixed = n_templates * n_chans * W * 4 + n_templates * 4
+    chans = np.uint32(n_chans)
+    per_second = chans * sampling_rate * 4
+    per_second += n_templates * sampling_rate * 4
+    per_second += (sampling_rate / W) * (5 * 4 + (groups / 3) * 4 + (groups / 3) * 4)
+    seconds = (budget - fixed) / per_second
+    seconds = min(seconds, np.floor(((1 << address_bits) - 1) / (4 * sampling_rate * chans)))
+    chunk = int(np.floor(seconds * sampling_rate))
+    if chunk < 4 * W:
+        raise ValueError("Cannot fit enough data on GPU to run binary pursuit. "
+                         "Decrease template samples or get a new GPU.")
+    onsets = []
+    onset = 0
+    while onset < n_samples - W:
+        onsets.append(onset)
+        onset += chunk - 3 * W
+    return onsets, chunk
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class _Pursuer:
+    """Device buffers and the C-ABI calls for one binary_pursuit() call."""
+
+    def __init__(self, torch, dev, n_chans, templates, bias, theta, W, S, max_chunk, flags,
+                 work_group_size):
+        self.torch = torch
+        self.dev = dev
+        self.C, self.W, self.S = n_chans, W, S
+        self.M = templates.shape[0]
+        self.flags = flags
+        self.wg = work_group_size
+        self.T = torch.from_numpy(np.ascontiguousarray(templates, dtype=np.float32)).to(dev)
+        self.bias = torch.from_numpy(np.ascontiguousarray(bias, dtype=np.float32)).to(dev)
+        self.theta = torch.from_numpy(np.ascontiguousarray(theta, dtype=np.float32)).to(dev)
+        d = _native.dims(n_chans, max_chunk, self.M, W, S, work_group_size)
+        nbytes = _native.workspace_bytes(d, flags)
+        if nbytes == 0:
+            raise ValueError("invalid binary pursuit sizes for the GPU library")
+        self.ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        self.stats = []
+
+    def chunk(self, host_chunk, clips):
+        torch = self.torch
+        C, N = host_chunk.shape
+        d = _native.dims(C, N, self.M, self.W, self.S, self.wg)
+        V = torch.from_numpy(host_chunk).to(self.dev)
+        nw = (N + self.W - 1) // self.W
+        cap = 4 * nw + 1024
+        stream = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        L = _native.lib()
+        while True:
+            idx = torch.empty(cap, dtype=torch.int32, device=self.dev)
+            lab = torch.empty(cap, dtype=torch.int32, device=self.dev)
+            n = ctypes.c_uint32(0)
+            st = _native.FbpChunkStats()
+            rc = L.fbp_pursue_chunk(ctypes.byref(d), self.flags, _ptr(V), _ptr(self.T),
+                                    _ptr(self.bias), _ptr(self.theta), _ptr(self.ws),
+                                    self.ws.numel(), _ptr(idx), _ptr(lab), cap, ctypes.byref(n),
+                                    ctypes.byref(st), 0, stream)
+            if rc == _native.FBP_E_CAPACITY:
+                cap *= 4
+                V.copy_(torch.from_numpy(host_chunk))
+                continue
+            _native.check(rc)
+            break
+        self.stats.append(st.as_dict())
+        k = n.value
+        out_clips = []
+        if clips and k > 0:
+            cl = torch.zeros((k, C * self.W), dtype=torch.float32, device=self.dev)
+            _native.check(L.fbp_adjusted_clips(ctypes.byref(d), _ptr(V), _ptr(self.T), _ptr(idx),
+                                               _ptr(lab), k, _ptr(cl), stream))
+            out_clips = cl.cpu().numpy()
+        si = idx[:k].cpu().numpy().view(np.uint32)
+        sl = lab[:k].cpu().numpy().view(np.uint32)
+        return si, sl, out_clips
+
+
+def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
+                   kernels_path=None, max_gpu_memory=None, *, mode="fast", device=None,
+                   work_group_size=WORK_GROUP_SIZE, verbose=True, return_stats=False):
+    """Find template spikes in ``voltage`` by binary pursuit on the GPU.
+
+    See the module docstring for the contract; the arguments mean what they
+    mean for the reference function (binary_pursuit_parallel.py:175-183)."""
+    import torch
+
+    del kernels_path
+    if not torch.cuda.is_available():
+        raise RuntimeError("No GPU available")
+    _native.lib()
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    n_chans = int(voltage.shape[0])
+    n_samples = int(voltage.shape[1])
+    sampling_rate = sort_info["sampling_rate"]
+    chan_win, _ = time_window_to_samples(sort_info["clip_width"], sampling_rate)
+    W = int(sort_info["n_samples_per_chan"])
+    templates = separability_metrics["templates"]
+    if templates.ndim == 1:
+        templates = np.reshape(templates, (1, -1))
+    templates = np.float32(templates)
+    M = templates.shape[0]
+    clip_init_samples = int(np.abs(chan_win[0]))
+    bias = np.float32(-0.5 * separability_metrics["template_SS"])
+    theta = np.float32(separability_metrics["neuron_lower_thresholds"])
+    if n_max_shift_inds is None or n_max_shift_inds < 0:
+        n_max_shift_inds = W // 2
+    S = int(np.uint32(n_max_shift_inds))
+    total_mem = torch.cuda.get_device_properties(dev).total_memory
+    onsets, chunk_len = plan_chunks(n_samples, n_chans, M, W, sampling_rate, S, total_mem,
+                                    max_gpu_memory, work_group_size)
+    flags = _native.FBP_OVERLAP_RECHECK if sort_info["do_overlap_recheck"] else 0
+    if mode == "plain":
+        flags |= _native.FBP_PLAIN_FP32
+    elif mode != "fast":
+        raise ValueError("mode must be 'fast' or 'plain'")
+    get_clips = bool(sort_info["get_adjusted_clips"])
+    idx_all, lab_all, bool_all, clips_all = [], [], [], []
+    pursuer = None
+    if onsets:
+        max_chunk = min(n_samples, chunk_len)
+        pursuer = _Pursuer(torch, dev, n_chans, templates, bias, theta, W, S, max_chunk, flags,
+                           work_group_size)
+    for start in onsets:
+        stop = int(np.uint32(min(n_samples, start + chunk_len)))
+        host_chunk = np.ascontiguousarray(np.float32(voltage[:, start:stop]))
+        si, sl, clips = pursuer.chunk(host_chunk, get_clips)
+        if si.size == 0:
+            continue
+        idx_all.append(si.astype(np.int64) + start)
+        lab_all.append(sl)
+        clips_all.append(clips)
+        bool_all.append(np.ones(si.size, dtype=bool))
+    if idx_all:
+        event_indices = np.int64(np.hstack(idx_all))
+        neuron_labels = np.int64(np.hstack(lab_all))
+        adjusted_clips = np.vstack(clips_all).astype(v_dtype)
+        spike_bool = np.hstack(bool_all)
+        event_indices += clip_init_samples
+        if verbose:
+            print("Found a total of", np.count_nonzero(spike_bool), "secret spikes", flush=True)
+    else:
+        event_indices, neuron_labels, spike_bool, adjusted_clips = [], [], [], []
+        if verbose:
+            print("Found a total of ZERO secret spikes", flush=True)
+    # side effect of add_n_spikes (neuron_separability.py:334-345)
+    labels_arr = np.asarray(neuron_labels)
+    separability_metrics["n_spikes"] = np.zeros(M)
+    for n in range(M):
+        separability_metrics["n_spikes"][n] = np.count_nonzero(labels_arr == n)
+    out = (event_indices, neuron_labels, spike_bool, adjusted_clips)
+    if return_stats:
+        return out, (pursuer.stats if pursuer else [])
+    return out

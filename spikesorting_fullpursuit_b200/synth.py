@@ -201,13 +201,17 @@ def make_recording(seed, n_chans=4, fs=40000, duration_s=1.0, n_units=6, layout=
         onset = times - pre
         ok = (onset >= 0) & (onset + W <= n_samples)
         onset, lab, sc = onset[ok], labels[ok], scales[ok]
-        T3 = templates.reshape(n_units, n_chans, W)
-        cols = onset[:, None] + np.arange(W)[None, :]
+        T3 = templates.reshape(n_units, n_chans, W).astype(np.float64)
+        taps = np.arange(W)
         for c in range(n_chans):
-            vals = sc[:, None] * T3[lab, c, :]
-            if not np.any(vals):
+            on_chan = np.flatnonzero(np.any(T3[:, c, :] != 0, axis=1))
+            sel = np.isin(lab, on_chan)
+            if not np.any(sel):
                 continue
-            np.add.at(voltage[c], cols.ravel(), vals.ravel().astype(np.float32))
+            cols = (onset[sel][:, None] + taps[None, :]).ravel()
+            vals = (sc[sel][:, None] * T3[lab[sel], c, :]).ravel()
+            add = np.bincount(cols, weights=vals, minlength=n_samples)
+            voltage[c] = (voltage[c] + add).astype(np.float32)
     sort_info = {
         "sampling_rate": fs,
         "clip_width": clip_width,

@@ -1,0 +1,102 @@
+"""Host-side checks that need no GPU: the C ABI loads and exports what
+include/fbp.h declares, argument validation, and the host logic shared with
+the oracle (chunk planner, clip window)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from spikesorting_fullpursuit_b200 import _native, build
+from spikesorting_fullpursuit_b200.overlap import binary_pursuit_parallel as bpp
+from spikesorting_fullpursuit_b200.processing.conversions import time_window_to_samples
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(_native.LIB_PATH):
+        build.build()
+    return _native.lib()
+
+
+def declared_functions():
+    src = open(os.path.join(REPO, "include", "fbp.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(fbp_\w+)\s*\(", src, re.M)))
+
+
+def test_header_declares_exports():
+    assert declared_functions() == sorted(_native.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    assert lib.fbp_abi_version() == 1
+
+
+def test_workspace_bytes(lib):
+    d = _native.dims(16, 400000, 40, 101, 100)
+    b = _native.workspace_bytes(d, _native.FBP_PLAIN_FP32)
+    assert b >= 40 * 400000 * 4
+    assert _native.workspace_bytes(d, 0) > b  # tensor-core buffers on top
+    bad = [_native.dims(0, 1000, 4, 101, 100), _native.dims(4, 100, 4, 101, 100),
+           _native.dims(4, 100000, 4, 101, 100, 100), _native.dims(4, 100000, 0, 101, 100),
+           _native.dims(4, 100000, 4, 2000, 100)]
+    for d in bad:
+        assert _native.workspace_bytes(d, 0) == 0
+
+
+def test_invalid_arguments_fail_before_any_device_call(lib):
+    d = _native.dims(4, 50, 4, 101, 100)
+    n = ctypes.c_uint32(0)
+    rc = lib.fbp_pursue_chunk(ctypes.byref(d), 0, None, None, None, None, None, 0, None, None, 0,
+                              ctypes.byref(n), None, 0, None)
+    assert rc == _native.FBP_E_ARG
+    assert b"invalid" in lib.fbp_last_error()
+    d = _native.dims(4, 5000, 4, 101, 100)
+    rc = lib.fbp_pursue_chunk(ctypes.byref(d), 0, None, None, None, None, None, 0, None, None, 0,
+                              ctypes.byref(n), None, 0, None)
+    assert rc == _native.FBP_E_ARG
+    buf = ctypes.c_void_p(1 << 40)
+    rc = lib.fbp_pursue_chunk(ctypes.byref(d), 0, buf, buf, buf, buf, buf, 16, buf, buf, 10,
+                              ctypes.byref(n), None, 0, None)
+    assert rc == _native.FBP_E_WORKSPACE
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_chunk_planner_matches_oracle(seed):
+    rng = np.random.default_rng(seed)
+    C = int(rng.integers(1, 70))
+    M = int(rng.integers(1, 250))
+    fs = int(rng.choice([20000, 30000, 40000]))
+    W = int(rng.integers(20, 130))
+    S = int(rng.integers(0, W + 5))
+    n = int(rng.integers(W + 1, 10 ** 8))
+    mem = int(rng.choice([8 * 1024 ** 3, 183 * 1024 ** 3, 48 * 1024 ** 3]))
+    mgm = None if rng.random() < 0.5 else int(rng.integers(10 ** 6, 10 ** 10))
+    try:
+        want = oracle.plan_chunks(n, C, M, W, fs, S, mem, mgm, 256)
+    except ValueError:
+        with pytest.raises(ValueError):
+            bpp.plan_chunks(n, C, M, W, fs, S, mem, mgm, 256)
+        return
+    assert bpp.plan_chunks(n, C, M, W, fs, S, mem, mgm, 256) == want
+
+
+@pytest.mark.parametrize("win", [[-1.0e-3, 1.5e-3], [1.0e-3, 1.5e-3], (-2.0e-4, 3.3e-4), [0.0, 0.0]])
+@pytest.mark.parametrize("fs", [30000, 40000, 24414.0625])
+def test_clip_window(win, fs):
+    assert time_window_to_samples(win, fs)[0] == oracle.time_window_to_samples(win, fs)[0]
+
+
+def test_product_does_not_import_oracle():
+    pkg = os.path.join(REPO, "spikesorting_fullpursuit_b200")
+    for root, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith(".py"):
+                src = open(os.path.join(root, f)).read()
+                assert "oracle" not in re.findall(r"^\s*(?:import|from)\s+(\w+)", src, re.M), f

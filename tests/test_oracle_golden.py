@@ -62,3 +62,20 @@ def test_oracle_chunk_internals(golden):
         assert int(st.spikes) == sum(ch["passes"])
         if ch["resid_sha256"] is not None:
             assert _sha(resid) == ch["resid_sha256"], name
+
+
+def test_reference_kernels_with_restated_host_loop(golden):
+    """oracle/ref_host.py (the CPU baseline of bench.py) reproduces the goldens."""
+    import os
+    import pytest
+    if not os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libbp_ref.so")):
+        pytest.skip("oracle/_ref not built")
+    import ref_host
+    name, V, si, sm, call, expect, meta = golden
+    ev, lab = ref_host.binary_pursuit(V, si, copy.deepcopy(sm), global_mem_size=meta["global_mem_size"],
+                                      work_group_size=meta["work_group_size"], **call)
+    if expect["empty"]:
+        assert ev.size == 0
+        return
+    assert _same(ev, expect["event_indices"]), name
+    assert _same(lab, expect["neuron_labels"]), name
