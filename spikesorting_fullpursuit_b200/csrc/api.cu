@@ -87,6 +87,21 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
         L->n_fix_cap = M * N / 4 + 4096;
         L->off_fix = take(L->n_fix_cap * 8);
     }
+    if (!(flags & FBP_PLAIN_FP32) && (flags & FBP_OVERLAP_RECHECK)) {
+        const uint64_t xt = M * M * S2 * S2 * 4;
+        if (xt <= (24ull << 30)) {  // larger template sets use the brute-force recheck
+            L->screened = true;
+            L->off_et = take(M * S2 * 8);
+            L->off_xt = take(xt);
+            uint64_t per = M * S2 * 4;
+            uint64_t gb = (1ull << 30) / per;
+            if (gb < 256) gb = 256;
+            if (gb > L->nw) gb = L->nw;
+            L->gbatch = gb;
+            L->off_g = take(gb * per);
+            L->off_perm = take(M * 4);
+        }
+    }
     L->bytes = align_up(off, 256);
     return true;
 }
@@ -183,6 +198,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         FBP_TRY(launch_tc_prepare_templates(d, w, templates, st));
         FBP_TRY(launch_tc_update_voltage(d, w, voltage, nullptr, nullptr, 0, true, st));
     }
+    if (!plain && overlap) FBP_TRY(launch_overlap_tables(d, w, templates, st));
     uint32_t nlist = d.nw, total = 0;
     api_detail::StageTimer tm;
     for (int32_t pass = 1;; ++pass) {
@@ -220,8 +236,6 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         FBP_CUDA(cudaStreamSynchronize(st));
         if (hs.error) return fail(FBP_E_DEVICE, "device status error");
         if (overlap) S.flagged += hs.n_flag;
-        S.fixups = hs.n_fix;
-        S.pair_exact = hs.n_pair_exact;
         const uint32_t n = hs.n_spikes;
         if (n == 0) break;
         if ((uint64_t)total + n > capacity) return fail(FBP_E_CAPACITY, "spike capacity exceeded");
@@ -247,7 +261,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     FBP_CUDA(cudaMemcpyAsync(&hs, w.status(), sizeof(hs), cudaMemcpyDeviceToHost, st));
     FBP_CUDA(cudaStreamSynchronize(st));
     S.fixups = hs.n_fix;
-    S.pair_exact = hs.pair_items;
+    S.pair_exact = (plain || !lay.screened) ? hs.pair_items : hs.n_pair_exact;
     S.n_spikes = total;
     *n_spikes = total;
     return FBP_OK;

@@ -51,6 +51,12 @@ struct Layout {
     // tensor-core likelihood (mode 1)
     size_t off_vt_hi, off_vt_lo, off_tt_hi, off_tt_lo, off_fix, off_tnorm;
     uint64_t Cp, Kt, Mp, n_fix_cap;
+    // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
+    // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
+    // template processing order perm[M]
+    size_t off_et, off_xt, off_g, off_perm;
+    uint64_t gbatch;
+    bool screened;
     size_t bytes;
 };
 
@@ -127,6 +133,7 @@ int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const
                              const uint32_t* win, uint32_t n, bool all, cudaStream_t st);
 
 // Screened overlap recheck (overlap_fast.cu)
+int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStream_t st);
 int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const float* T,
                         const float* theta, uint32_t nflag_max, cudaStream_t st);
 

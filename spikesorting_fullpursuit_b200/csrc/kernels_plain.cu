@@ -341,7 +341,6 @@ __global__ void __launch_bounds__(kOvThreads) overlap_plain_kernel(
     typedef cub::BlockScan<uint32_t, kOvThreads> Scan;
     __shared__ typename Scan::TempStorage scan_tmp;
     __shared__ unsigned long long s_best;
-    __shared__ uint32_t s_ncand;
     extern __shared__ __align__(16) float sm[];
     const uint32_t S = d.S, W = d.W, C = d.C;
     const uint32_t S2 = 2 * S + 1;
@@ -626,7 +625,6 @@ struct AcceptCtx {
     const uint32_t* best_idx;
     const float* theta;
 
-    __device__ uint32_t id(uint32_t k) const { return list[k]; }
     __device__ bool at(int64_t k, uint32_t x) const { return k >= 0 && k < (int64_t)n && list[k] == x; }
     __device__ bool same_group(uint32_t a, uint32_t b) const { return a / d.WG == b / d.WG; }
     // does the accept of the window at position kk write 3 into check[x]?
