@@ -78,13 +78,13 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
         L->Cp = (C + 7) / 8 * 8;
         L->Kt = W;
         L->Mp = (M + 15) / 16 * 16;
-        const uint64_t rows = N + 256 + 2 * W;
-        L->off_vt_hi = take(rows * L->Cp * 2);
-        L->off_vt_lo = take(rows * L->Cp * 2);
-        L->off_tt_hi = take(L->Mp * W * L->Cp * 2);
-        L->off_tt_lo = take(L->Mp * W * L->Cp * 2);
+        L->vq_rows = N + 256 + 2 * W;
+        L->off_vt_hi = take(L->vq_rows * L->Cp * 4);   // voltage as [Cp/4][rows][4] fp32
+        L->off_tt_hi = take(L->Mp * W * L->Cp * 4);    // templates as [W][Cp/8][2][Mp][4] fp32
         L->off_tnorm = take(M * C * 4);
-        L->n_fix_cap = M * N / 4 + 4096;
+        uint64_t cap = M * N / 4;
+        if (cap > (32ull << 20)) cap = 32ull << 20;
+        L->n_fix_cap = cap + 4096;
         L->off_fix = take(L->n_fix_cap * 8);
     }
     if (!(flags & FBP_PLAIN_FP32) && (flags & FBP_OVERLAP_RECHECK)) {
@@ -234,8 +234,9 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         DevStatus hs;
         FBP_CUDA(cudaMemcpyAsync(&hs, w.status(), sizeof(hs), cudaMemcpyDeviceToHost, st));
         FBP_CUDA(cudaStreamSynchronize(st));
-        if (hs.error) return fail(FBP_E_DEVICE, "device status error");
+        if (hs.error) return fail(FBP_E_DEVICE, "device status error " + std::to_string(hs.error));
         if (overlap) S.flagged += hs.n_flag;
+        S.fixups += hs.n_fix;
         const uint32_t n = hs.n_spikes;
         if (n == 0) break;
         if ((uint64_t)total + n > capacity) return fail(FBP_E_CAPACITY, "spike capacity exceeded");
@@ -260,7 +261,6 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     DevStatus hs;
     FBP_CUDA(cudaMemcpyAsync(&hs, w.status(), sizeof(hs), cudaMemcpyDeviceToHost, st));
     FBP_CUDA(cudaStreamSynchronize(st));
-    S.fixups = hs.n_fix;
     S.pair_exact = (plain || !lay.screened) ? hs.pair_items : hs.n_pair_exact;
     S.n_spikes = total;
     *n_spikes = total;

@@ -50,7 +50,7 @@ struct Layout {
     size_t off_blk, off_status;
     // tensor-core likelihood (mode 1)
     size_t off_vt_hi, off_vt_lo, off_tt_hi, off_tt_lo, off_fix, off_tnorm;
-    uint64_t Cp, Kt, Mp, n_fix_cap;
+    uint64_t Cp, Kt, Mp, n_fix_cap, vq_rows;
     // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
     // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
     // template processing order perm[M]

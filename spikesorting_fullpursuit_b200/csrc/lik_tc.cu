@@ -1,21 +1,515 @@
-// lik_tc.cu -- tensor-core likelihood (filled in after the exact path).
+// lik_tc.cu -- template-by-voltage likelihood on the 5th-generation tensor cores.
+//
+// L[t][s] = bias[t] + sum_c sum_j T[t][c][j] V[c][s+j]  (compute_full_likelihood,
+// binary_pursuit.cl:216-300) as a GEMM over K = (tap j, channel c):
+//   A[s][(j,c)] = V[c][s+j]   -- a Hankel matrix of the voltage
+//   B[(j,c)][t] = T[t][c][j]
+// with tcgen05.mma kind::tf32, M = 128 samples per tile, N = templates, K = 8
+// channels per instruction, FP32 accumulators in TMEM.
+//
+// The voltage is kept on the device as Vq[Cp/4][rows][4] (four channels per
+// 16-byte row).  A tile's strip of rows [s0, s0+128+W-1) is copied into shared
+// memory once with cp.async.bulk; the UMMA operand for tap j is the same strip
+// seen from row j, i.e. the shared-memory descriptor's start address advanced by
+// 16*j bytes (canonical K-major layout without swizzle: 8-row core matrices of
+// 16-byte rows).  No Hankel expansion is ever materialised.  Templates are
+// pre-arranged as Tq[j][Cp/8][2][Np][4] and streamed per (tap, channel pair)
+// through a ring of shared-memory stages.
+//
+// Exactness.  The pursuit reads a likelihood either for its sign or, when it is
+// positive, for its value.  The epilogue bounds |estimate - reference float
+// result| rigorously (TF32 operand truncation, FP32 accumulation, the
+// reference's own sequential rounding), stores the estimate wherever
+// estimate + bound <= 0, and queues every other sample for an exact FP32
+// recomputation in the reference order (fixup kernel).  The stored likelihood
+// therefore equals the reference's wherever the reference's is positive and is
+// <= 0 wherever the reference's is <= 0.
+//
+// Roles of the 6 warps of a CTA: warp 0 lane 0 issues the bulk copies, warp 1
+// allocates TMEM and lane 0 issues the MMAs, warps 2-5 run the epilogue (warp w
+// reads TMEM lanes 32*(w%4) .. +32).  Every mbarrier wait is bounded; on a
+// timeout the kernel records an error in the status word and returns after
+// draining its own operations.
+#include <cub/cub.cuh>
+
 #include "fbp_internal.cuh"
 
 namespace fbp {
+namespace {
 
-bool tc_supported(const Dims&) { return false; }
+constexpr int kTile = 128;         // samples per UMMA tile (M)
+constexpr int kThreads = 192;
+constexpr uint32_t kSpin = 1u << 24;
 
-int launch_likelihood_tc(const Dims&, const Work&, const float*, const float*, const float*,
-                         const uint32_t*, uint32_t, float*, bool, cudaStream_t, uint64_t*)
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
-    return fail(FBP_E_ARG, "tensor-core likelihood not available");
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-int launch_tc_prepare_templates(const Dims&, const Work&, const float*, cudaStream_t) { return FBP_OK; }
-
-int launch_tc_update_voltage(const Dims&, const Work&, const float*, const uint32_t*, const uint32_t*,
-                             uint32_t, bool, cudaStream_t)
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
 {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after kSpin unsuccessful polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < kSpin; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    // canonical K-major, no swizzle; version 1 (sm_100) at bit 46
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct TcParams {
+    Dims d;
+    const float* V;       // [C][N] (exact recomputation)
+    const float* T;       // [M][C][W]
+    const float* Vq;      // [Cq][rows][4]
+    const float* Tq;      // [W][Cq/2][2][Np][4]
+    const float* bias;    // [M]
+    const float* tnorm;   // [M][C] channel norms of the templates
+    const uint32_t* list; // listed windows (mode 1) or null (mode 0: contiguous tiles)
+    uint32_t nitems;      // tiles (mode 0) or listed windows (mode 1)
+    uint32_t rows;        // rows of each Vq channel block
+    uint32_t Cq, Np, ntiles, R8, stages, ncols;
+    float* L;
+    unsigned long long* fix;
+    uint32_t fix_cap;
+    DevStatus* status;
+    float k_a, k_b;       // bound = k_a * sum_c |T_tc| |V_c strip| + k_b * |bias_t|
+};
+
+__device__ float exact_likelihood(const Dims& d, const float* __restrict__ V, const float* __restrict__ T,
+                                  float b, uint32_t t, uint32_t s)
+{
+    float acc = b;
+    for (uint32_t c = 0; c < d.C; ++c) {
+        const float* tr = T + ((uint64_t)t * d.C + c) * d.W;
+        const float* vr = V + (uint64_t)c * d.N + s;
+        for (uint32_t j = 0; j < d.W; ++j) acc = __fadd_rn(acc, __fmul_rn(tr[j], vr[j]));
+    }
+    return acc;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const Dims& d = P.d;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t strip_bytes = P.R8 * 16;                  // one 4-channel block of a tile strip
+    const uint32_t tile_bytes = P.Cq * strip_bytes;
+    const uint32_t stage_bytes = P.Np * 32;                  // one (tap, channel pair) of templates
+    unsigned char* A = smem;
+    unsigned char* B = A + P.ntiles * tile_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(B + P.stages * stage_bytes);
+    uint64_t* a_full = bars;
+    uint64_t* acc_full = bars + 1;
+    uint64_t* b_full = bars + 2;
+    uint64_t* b_empty = b_full + P.stages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(b_empty + P.stages);
+    uint32_t* err = tmem_slot + 1;
+    uint32_t* t_s0 = err + 1;                                // [ntiles]
+    uint32_t* t_rows = t_s0 + P.ntiles;                      // [ntiles]
+    float* snorm = reinterpret_cast<float*>(t_rows + P.ntiles);   // [ntiles][C]
+    float* bnd = snorm + P.ntiles * d.C;                          // [ntiles][M]
+
+    const uint32_t ksteps = d.W * (P.Cq / 2);
+    if (threadIdx.x == 0) {
+        mbar_init(a_full, 1);
+        mbar_init(acc_full, 1);
+        for (uint32_t s = 0; s < P.stages; ++s) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1);
+        }
+        *err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (threadIdx.x < P.ntiles) {
+        const uint32_t i = threadIdx.x;
+        const uint64_t item = (uint64_t)blockIdx.x * P.ntiles + i;
+        uint32_t s0 = 0, rows = 0;
+        if (P.list == nullptr) {
+            const uint64_t st = item * kTile;
+            if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)kTile ? d.N - st : (uint64_t)kTile); }
+        } else if (item < P.nitems) {
+            const uint64_t st = (uint64_t)P.list[item] * d.W;
+            if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)d.W ? d.N - st : (uint64_t)d.W); }
+        }
+        t_s0[i] = s0;
+        t_rows[i] = rows;
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(P.ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // voltage strips, one bulk copy per tile and 4-channel block
+            mbar_expect_tx(a_full, P.ntiles * tile_bytes);
+            for (uint32_t i = 0; i < P.ntiles; ++i)
+                for (uint32_t q = 0; q < P.Cq; ++q)
+                    bulk_g2s(A + i * tile_bytes + q * strip_bytes,
+                             P.Vq + ((uint64_t)q * P.rows + t_s0[i]) * 4, strip_bytes, a_full);
+            // templates, one stage per (tap, channel pair)
+            for (uint32_t k = 0; k < ksteps; ++k) {
+                const uint32_t st = k % P.stages, round = k / P.stages;
+                if (round > 0 && !mbar_wait(&b_empty[st], (round - 1) & 1)) { atomicOr(err, 1u); break; }
+                mbar_expect_tx(&b_full[st], stage_bytes);
+                bulk_g2s(B + st * stage_bytes, P.Tq + (uint64_t)k * P.Np * 8, stage_bytes, &b_full[st]);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((P.Np >> 3) << 17) | ((kTile >> 4) << 24);
+            bool ok = mbar_wait(a_full, 0);
+            const uint32_t a_base = smem_u32(A), b_base = smem_u32(B);
+            uint32_t issued = 0;
+            for (uint32_t k = 0; ok && k < ksteps; ++k) {
+                const uint32_t st = k % P.stages, round = k / P.stages;
+                if (!mbar_wait(&b_full[st], round & 1)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t j = k / (P.Cq / 2), qp = k % (P.Cq / 2);
+                const uint64_t bdesc = umma_desc(b_base + st * stage_bytes, P.Np * 16, 128);
+                for (uint32_t i = 0; i < P.ntiles; ++i) {
+                    const uint32_t a_addr = a_base + i * tile_bytes + (2 * qp) * strip_bytes + j * 16;
+                    const uint64_t adesc = umma_desc(a_addr, strip_bytes, 128);
+                    umma_tf32(tmem + i * P.Np, adesc, bdesc, idesc, k > 0 ? 1u : 0u);
+                }
+                umma_commit(&b_empty[st]);
+                ++issued;
+            }
+            if (!ok) atomicOr(err, 2u);
+            umma_commit(acc_full);   // arrives once every MMA issued above has completed
+        }
+    } else {
+        // epilogue warps 2..5
+        const uint32_t et = threadIdx.x - 64;
+        const bool a_ok = mbar_wait(a_full, 0);
+        if (a_ok) {
+            // per-tile channel norms of the voltage strip (rows [0, rows+W-1))
+            for (uint32_t e = et; e < P.ntiles * d.C; e += 128) {
+                const uint32_t i = e / d.C, c = e % d.C;
+                const float* col = reinterpret_cast<const float*>(A + i * tile_bytes + (c / 4) * strip_bytes) + (c % 4);
+                const uint32_t nr = t_rows[i] ? t_rows[i] + d.W - 1 : 0;
+                float acc = 0.f;
+                for (uint32_t r = 0; r < nr; ++r) acc = fmaf(col[r * 4], col[r * 4], acc);
+                snorm[e] = sqrtf(acc) * 1.0001f;
+            }
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        for (uint32_t e = et; e < P.ntiles * d.M; e += 128) {
+            const uint32_t i = e / d.M, t = e % d.M;
+            float a = 0.f;
+            for (uint32_t c = 0; c < d.C; ++c) a = fmaf(P.tnorm[t * d.C + c], snorm[i * d.C + c], a);
+            bnd[e] = P.k_a * a * 1.0001f + P.k_b * fabsf(P.bias[t]);
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        const bool acc_ok = a_ok && mbar_wait(acc_full, 0);
+        tc_fence_after();
+        if (!acc_ok) {
+            if (et == 0) atomicOr(err, 4u);
+        } else {
+            const uint32_t qd = warp & 3;
+            const uint32_t row = qd * 32 + lane;
+            for (uint32_t i = 0; i < P.ntiles; ++i) {
+                const uint32_t s = t_s0[i] + row;
+                const bool valid = row < t_rows[i];
+                for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
+                    float v[16];
+                    tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
+                    if (!valid) continue;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const uint32_t t = cg * 16 + e;
+                        if (t >= d.M) continue;
+                        float out;
+                        if ((uint64_t)s + d.W >= d.N) {
+                            out = 0.f;
+                        } else {
+                            const float b = P.bias[t];
+                            const float est = v[e] + b;
+                            out = est;
+                            if (!(est + bnd[i * d.M + t] <= 0.f)) {
+                                const uint32_t slot = atomicAdd(&P.status->n_fix, 1u);
+                                if (slot < P.fix_cap)
+                                    P.fix[slot] = ((unsigned long long)t << 32) | s;
+                                else
+                                    out = exact_likelihood(d, P.V, P.T, b, t, s);
+                            }
+                        }
+                        P.L[(uint64_t)t * d.N + s] = out;
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *err) atomicOr(&P.status->error, 0x100u | *err);
+    if (warp == 1) {
+        // drain: the accumulator barrier completes once all issued MMAs are done
+        if (lane == 0 && (*err & 4u)) mbar_wait(acc_full, 0);
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
+    }
+}
+
+// Exact recomputation of the queued samples (reference order, FP32).
+__global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
+                             const float* __restrict__ bias, const unsigned long long* __restrict__ fix,
+                             uint32_t cap, const DevStatus* status, float* L)
+{
+    const uint32_t n = min(status->n_fix, cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long e = fix[i];
+        const uint32_t t = (uint32_t)(e >> 32), s = (uint32_t)(e & 0xFFFFFFFFu);
+        L[(uint64_t)t * d.N + s] = exact_likelihood(d, V, T, bias[t], t, s);
+    }
+}
+
+// Vq[q][r][e] = V[4q+e][r] for r < N (zero elsewhere and for padding channels).
+__global__ void voltage_pack_kernel(Dims d, const float* __restrict__ V, uint32_t Cq, uint32_t rows, float4* Vq)
+{
+    const uint64_t total = (uint64_t)Cq * rows;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t q = (uint32_t)(i / rows), r = (uint32_t)(i % rows);
+        float x[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t c = 4 * q + e;
+            x[e] = (r < d.N && c < d.C) ? V[(uint64_t)c * d.N + r] : 0.f;
+        }
+        Vq[i] = make_float4(x[0], x[1], x[2], x[3]);
+    }
+}
+
+// Refresh Vq on the rows touched by the spikes of a pass.
+__global__ void voltage_repack_kernel(Dims d, const float* __restrict__ V, uint32_t Cq, uint32_t rows,
+                                      const uint32_t* __restrict__ idx, uint32_t n, float4* Vq)
+{
+    for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const uint32_t s = idx[k];
+        for (uint32_t e2 = threadIdx.x; e2 < Cq * d.W; e2 += blockDim.x) {
+            const uint32_t q = e2 / d.W, r = s + e2 % d.W;
+            if (r >= d.N) continue;
+            float x[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t c = 4 * q + e;
+                x[e] = c < d.C ? V[(uint64_t)c * d.N + r] : 0.f;
+            }
+            Vq[(uint64_t)q * rows + r] = make_float4(x[0], x[1], x[2], x[3]);
+        }
+    }
+}
+
+// Tq[j][qp][h][n][e] = T[n][(2qp+h)*4+e][j]; tnorm[t][c] = |T[t][c][:]|.
+__global__ void template_pack_kernel(Dims d, const float* __restrict__ T, uint32_t Cq, uint32_t Np, float* Tq,
+                                     float* tnorm)
+{
+    const uint64_t total = (uint64_t)d.W * Cq * Np * 4;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t e = i % 4;
+        const uint32_t n = (i / 4) % Np;
+        const uint32_t qh = (uint32_t)((i / 4 / Np) % Cq);   // = 2*qp + h
+        const uint32_t j = (uint32_t)(i / 4 / Np / Cq);
+        const uint32_t c = qh * 4 + e;
+        Tq[i] = (n < d.M && c < d.C) ? T[((uint64_t)n * d.C + c) * d.W + j] : 0.f;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.M * d.C; i += gridDim.x * blockDim.x) {
+        const float* r = T + (uint64_t)i * d.W;
+        double a = 0.0;
+        for (uint32_t j = 0; j < d.W; ++j) a += (double)r[j] * r[j];
+        tnorm[i] = (float)(sqrt(a) * (1.0 + 1e-6));
+    }
+}
+
+struct TcConfig {
+    uint32_t Cq, Np, ntiles, R8, stages, ncols;
+    size_t smem;
+};
+
+bool tc_config(const Dims& d, TcConfig* c)
+{
+    if (d.W > (uint32_t)kTile || d.W == 0) return false;
+    const uint32_t Cp = (d.C + 7) / 8 * 8;
+    c->Cq = Cp / 4;
+    c->Np = (d.M + 15) / 16 * 16;
+    if (c->Np > 256) return false;
+    c->R8 = (kTile + d.W - 1 + 7) / 8 * 8;
+    c->ntiles = 512 / c->Np;
+    if (c->ntiles > 4) c->ntiles = 4;
+    if (c->ntiles == 0) return false;
+    for (;;) {
+        const uint32_t cols = c->ntiles * c->Np;
+        c->ncols = 32;
+        while (c->ncols < cols) c->ncols <<= 1;
+        const size_t strips = (size_t)c->ntiles * c->Cq * c->R8 * 16;
+        const size_t stage = (size_t)c->Np * 32;
+        c->stages = 8;
+        while (c->stages > 2 && strips + c->stages * stage > 160 * 1024) c->stages >>= 1;
+        c->smem = strips + c->stages * stage + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
+                  (size_t)c->ntiles * (d.C + d.M) * 4 + 1024;
+        if (c->smem <= 200 * 1024) return true;
+        if (c->ntiles == 1) return false;
+        --c->ntiles;
+    }
+}
+
+}  // namespace
+
+bool tc_supported(const Dims& d)
+{
+    TcConfig c;
+    return tc_config(d, &c);
+}
+
+int launch_tc_prepare_templates(const Dims& d, const Work& w, const float* T, cudaStream_t st)
+{
+    TcConfig c;
+    if (!tc_config(d, &c)) return FBP_OK;
+    const Layout& L = *w.lay;
+    template_pack_kernel<<<256, 256, 0, st>>>(d, T, c.Cq, c.Np, w.at<float>(L.off_tt_hi), w.at<float>(L.off_tnorm));
+    FBP_CUDA(cudaGetLastError());
+    return FBP_OK;
+}
+
+int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const uint32_t* idx, const uint32_t* win,
+                             uint32_t n, bool all, cudaStream_t st)
+{
+    (void)win;
+    TcConfig c;
+    if (!tc_config(d, &c)) return FBP_OK;
+    const Layout& L = *w.lay;
+    float4* Vq = w.at<float4>(L.off_vt_hi);
+    if (all) {
+        voltage_pack_kernel<<<148 * 16, 256, 0, st>>>(d, V, c.Cq, (uint32_t)L.vq_rows, Vq);
+    } else if (n > 0) {
+        voltage_repack_kernel<<<n < 65535u ? n : 65535u, 128, 0, st>>>(d, V, c.Cq, (uint32_t)L.vq_rows, idx, n, Vq);
+    }
+    FBP_CUDA(cudaGetLastError());
+    return FBP_OK;
+}
+
+int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T, const float* bias,
+                         const uint32_t* list, uint32_t nlist, float* Lk, bool refresh_voltage, cudaStream_t st,
+                         uint64_t* n_fix_out)
+{
+    (void)refresh_voltage;
+    (void)n_fix_out;
+    if (nlist == 0) return FBP_OK;
+    TcConfig c;
+    if (!tc_config(d, &c)) return fail(FBP_E_ARG, "tensor-core likelihood not supported for these sizes");
+    const Layout& L = *w.lay;
+    TcParams P;
+    P.d = d;
+    P.V = V;
+    P.T = T;
+    P.Vq = w.at<float>(L.off_vt_hi);
+    P.Tq = w.at<float>(L.off_tt_hi);
+    P.bias = bias;
+    P.tnorm = w.at<float>(L.off_tnorm);
+    const bool all = nlist == d.nw;
+    P.list = all ? nullptr : list;
+    const uint64_t items = all ? ((uint64_t)d.N + kTile - 1) / kTile : nlist;
+    P.nitems = (uint32_t)items;
+    P.rows = (uint32_t)L.vq_rows;
+    P.Cq = c.Cq;
+    P.Np = c.Np;
+    P.ntiles = c.ntiles;
+    P.R8 = c.R8;
+    P.stages = c.stages;
+    P.ncols = c.ncols;
+    P.L = Lk;
+    P.fix = w.at<unsigned long long>(L.off_fix);
+    P.fix_cap = (uint32_t)L.n_fix_cap;
+    P.status = w.status();
+    // |tf32 operands| rel. error < 2^-10 each -> products < 2^-9; FP32 accumulation of n terms
+    // (any order, truncating) < n 2^-22; the reference's sequential float sum < (n+1) 2^-24.
+    const double n = (double)d.C * d.W;
+    const double u24 = 1.0 / 16777216.0;
+    P.k_a = (float)(1.1 * (1.0 / 512.0 + (2.0 * n + 8.0) * 4.0 * u24 + (n + 2.0) * u24));
+    P.k_b = (float)(1.1 * (n + 8.0) * 4.0 * u24);
+    FBP_CUDA(cudaMemsetAsync(&w.status()->n_fix, 0, 4, st));
+    FBP_CUDA(cudaFuncSetAttribute(lik_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+    const uint32_t grid = (uint32_t)((items + c.ntiles - 1) / c.ntiles);
+    lik_tc_kernel<<<grid, kThreads, c.smem, st>>>(P);
+    fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, bias, P.fix, P.fix_cap, w.status(), Lk);
+    FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }
 
