@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-s", type=float, default=2.0)
+    p.add_argument("--only-device", action="store_true",
+                   help="time the device-resident steps only (no e2e, plain, stage or CPU legs); for profiling")
     return p.parse_args()
 
 
@@ -235,6 +237,16 @@ def main():
         t_fast = float(t.item())
     units = C * N * args.steps * world
     value = units / (t_fast * 1e-3) / 1e6
+    if args.only_device:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "Msample*ch/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fast / args.steps,
+                              "config": {"workload": args.config, "samples": N, "channels": C},
+                              "stats": st_fast, "clocks": clocks}), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     # per-stage breakdown (separate untimed run with stage events)
     _, st_stage, _ = run_mode(0, 1, 0, timing=True)
 

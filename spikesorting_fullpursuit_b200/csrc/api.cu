@@ -100,6 +100,7 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
             L->gbatch = gb;
             L->off_g = take(gb * per);
             L->off_perm = take(M * 4);
+            L->off_mx = take(M * M * 4 + 2 * M * 4);   // max -X_ft per pair; max sqrt(E), max E per template
         }
     }
     L->bytes = align_up(off, 256);

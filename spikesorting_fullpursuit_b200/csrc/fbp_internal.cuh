@@ -54,7 +54,7 @@ struct Layout {
     // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
     // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
     // template processing order perm[M]
-    size_t off_et, off_xt, off_g, off_perm;
+    size_t off_et, off_xt, off_g, off_perm, off_mx;
     uint64_t gbatch;
     bool screened;
     size_t bytes;

@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
     uint32_t* t_rows = t_s0 + P.ntiles;                      // [ntiles]
     float* snorm = reinterpret_cast<float*>(t_rows + P.ntiles);   // [ntiles][C]
     float* bnd = snorm + P.ntiles * d.C;                          // [ntiles][M]
+    float* sbias = bnd + P.ntiles * d.M;                          // [M]
 
     const uint32_t ksteps = d.W * (P.Cq / 2);
     if (threadIdx.x == 0) {
@@ -270,6 +271,7 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
             }
         }
         asm volatile("bar.sync 1, 128;" ::: "memory");
+        for (uint32_t t = et; t < d.M; t += 128) sbias[t] = P.bias[t];
         for (uint32_t e = et; e < P.ntiles * d.M; e += 128) {
             const uint32_t i = e / d.M, t = e % d.M;
             float a = 0.f;
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
                         if ((uint64_t)s + d.W >= d.N) {
                             out = 0.f;
                         } else {
-                            const float b = P.bias[t];
+                            const float b = sbias[t];
                             const float est = v[e] + b;
                             out = est;
                             if (!(est + bnd[i * d.M + t] <= 0.f)) {
@@ -423,7 +425,7 @@ bool tc_config(const Dims& d, TcConfig* c)
         c->stages = 8;
         while (c->stages > 2 && strips + c->stages * stage > 160 * 1024) c->stages >>= 1;
         c->smem = strips + c->stages * stage + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
-                  (size_t)c->ntiles * (d.C + d.M) * 4 + 1024;
+                  (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + 1024;
         if (c->smem <= 200 * 1024) return true;
         if (c->ntiles == 1) return false;
         --c->ntiles;

@@ -27,8 +27,10 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 
 // Truncated energy of template t at shift x: sum over the template samples u
-// that land inside the window, u in [S-x, S-x+W) and [0, W).
-__global__ void energy_table_kernel(Dims d, const float* __restrict__ T, double* Et)
+// that land inside the window, u in [S-x, S-x+W) and [0, W).  Stored as
+// (E, sqrt(E)), each rounded up, for the screening bound and the partial
+// correlations.
+__global__ void energy_table_kernel(Dims d, const float* __restrict__ T, float2* Et)
 {
     const uint32_t S2 = 2 * d.S + 1;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.M * S2; i += gridDim.x * blockDim.x) {
@@ -39,7 +41,7 @@ __global__ void energy_table_kernel(Dims d, const float* __restrict__ T, double*
             const float* r = T + ((uint64_t)t * d.C + c) * d.W;
             for (int u = lo; u < hi; ++u) e += (double)r[u] * (double)r[u];
         }
-        Et[i] = e;
+        Et[i] = make_float2(__double2float_ru(e * (1.0 + 1e-12)), __double2float_ru(sqrt(e) * (1.0 + 1e-12)));
     }
 }
 
@@ -48,8 +50,12 @@ __global__ void energy_table_kernel(Dims d, const float* __restrict__ T, double*
 // X_ft(a, b) = Q_delta[hi] - Q_delta[lo] with delta = a-b.
 constexpr int kLagChunk = 16;
 
-__global__ void __launch_bounds__(256) cross_table_kernel(Dims d, const float* __restrict__ T, float* XT)
+__global__ void __launch_bounds__(256) cross_table_kernel(Dims d, const float* __restrict__ T, float* XT,
+                                                          float* max_negx)
 {
+    typedef cub::BlockReduce<float, 256> RF;
+    __shared__ typename RF::TempStorage rtmp;
+    float mneg = 0.f;
     extern __shared__ __align__(16) unsigned char smraw[];
     const uint32_t f = blockIdx.x / d.M, t = blockIdx.x % d.M;
     const uint32_t S2 = 2 * d.S + 1, W = d.W, C = d.C;
@@ -84,9 +90,28 @@ __global__ void __launch_bounds__(256) cross_table_kernel(Dims d, const float* _
             const int lo = max(max(0, -delta), (int)d.S - a);
             const int hi = min(min((int)W, (int)W - delta), (int)d.S - a + (int)W);
             const double v = hi > lo ? Q[li * (W + 1) + hi] - Q[li * (W + 1) + lo] : 0.0;
-            XT[(((uint64_t)f * d.M + t) * S2 + a) * S2 + b] = (float)v;
+            const float xv = (float)v;
+            XT[(((uint64_t)f * d.M + t) * S2 + a) * S2 + b] = xv;
+            mneg = fmaxf(mneg, -xv);
         }
         __syncthreads();
+    }
+    const float m = RF(rtmp).Reduce(mneg, cub::Max());
+    if (threadIdx.x == 0) max_negx[blockIdx.x] = m;
+}
+
+// Per template: max over shifts of sqrt(E) and of E (bounds for whole rows).
+__global__ void energy_max_kernel(Dims d, const float2* __restrict__ Et, float* maxs)
+{
+    const uint32_t S2 = 2 * d.S + 1;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < d.M; t += gridDim.x * blockDim.x) {
+        float ms = 0.f, me = 0.f;
+        for (uint32_t x = 0; x < S2; ++x) {
+            ms = fmaxf(ms, Et[(uint64_t)t * S2 + x].y);
+            me = fmaxf(me, Et[(uint64_t)t * S2 + x].x);
+        }
+        maxs[t] = ms;
+        maxs[d.M + t] = me;
     }
 }
 
@@ -128,7 +153,7 @@ __global__ void __launch_bounds__(1024) partial_corr_kernel(Dims d, const float*
                                                             const float* __restrict__ T,
                                                             const float* __restrict__ L,
                                                             const float* __restrict__ theta,
-                                                            const double* __restrict__ Et,
+                                                            const float2* __restrict__ Et,
                                                             const uint32_t* __restrict__ perm,
                                                             const uint32_t* __restrict__ flag,
                                                             const DevStatus* status,
@@ -203,26 +228,29 @@ __global__ void __launch_bounds__(1024) partial_corr_kernel(Dims d, const float*
         const uint32_t gi = g0 + q;
         if (gi < d.M) {
             const uint32_t t = perm[gi];
-            Gk[(uint64_t)t * S2 + b] = (float)((double)acc[q] - 0.5 * Et[(uint64_t)t * S2 + b]);
+            Gk[(uint64_t)t * S2 + b] = acc[q] - 0.5f * Et[(uint64_t)t * S2 + b].x;
         }
     }
 }
 
-// Exact pair likelihood in the reference's float order (binary_pursuit.cl:578-632).
-__device__ float pair_exact(const Dims& d, const float* __restrict__ T, const float* __restrict__ V,
-                            uint32_t f, uint32_t t, uint32_t p, uint32_t a, uint32_t b)
+// Exact pair likelihood in the reference's float order (binary_pursuit.cl:578-632),
+// with the window's voltage vw[C][W] in shared memory.
+__device__ float pair_exact_sv(const Dims& d, const float* __restrict__ T, const float* vw, uint32_t f, uint32_t t,
+                               uint32_t a, uint32_t b)
 {
     const int W = (int)d.W, fa = (int)d.S - (int)a, ta = (int)d.S - (int)b;
+    const int jlo_f = max(0, -fa), jhi_f = min(W, W - fa);
+    const int jlo_t = max(0, -ta), jhi_t = min(W, W - ta);
     float acc = 0.f;
     for (uint32_t c = 0; c < d.C; ++c) {
-        const float* fr = T + ((uint64_t)f * d.C + c) * d.W;
-        const float* tr = T + ((uint64_t)t * d.C + c) * d.W;
-        const float* vr = V + (uint64_t)c * d.N + p;
+        const float* fr = T + ((uint64_t)f * d.C + c) * d.W + fa;
+        const float* tr = T + ((uint64_t)t * d.C + c) * d.W + ta;
+        const float* vr = vw + c * d.W;
         float ss = 0.f;
+#pragma unroll 4
         for (int j = 0; j < W; ++j) {
-            const int xf = fa + j, xt = ta + j;
-            const float fv = (xf >= 0 && xf < W) ? fr[xf] : 0.f;
-            const float tv = (xt >= 0 && xt < W) ? tr[xt] : 0.f;
+            const float fv = (j >= jlo_f && j < jhi_f) ? __ldg(fr + j) : 0.f;
+            const float tv = (j >= jlo_t && j < jhi_t) ? __ldg(tr + j) : 0.f;
             const float s = fadd(fv, tv);
             ss = fadd(ss, fmul(s, s));
             acc = fadd(acc, fmul(s, vr[j]));
@@ -240,43 +268,56 @@ __device__ __forceinline__ uint32_t item_priority(uint64_t r, uint32_t WG, uint3
 }
 
 constexpr int kScrThreads = 256;
+constexpr int kRowCap = 8192;   // per-row upper bounds kept in shared memory
+constexpr int kCandCap = 2048;  // exact-scoring candidates per window pass
 
 struct ScreenShared {
-    double lb;
-    double nv;
+    float lb;
+    float nv;
     unsigned long long best;
     uint32_t nA;
     uint32_t nTB;
 };
 
-// Screening of one flagged window per CTA.
+// Screening of one flagged window per CTA.  Items are enumerated as rows:
+// part 1 = (a in A+, t) rows over all b; part 2 = ((t, b) with L_t > 0) rows
+// over the a not in A+.  A warp handles a row, lanes the varying shift.
+// Pass 1 gives the lower bound LB = max(est - bound) and per-row maxima of
+// est + bound; pass 2 revisits only rows that can reach max(LB, seed) and
+// scores their candidates exactly.
 __global__ void __launch_bounds__(kScrThreads) screen_kernel(
     Dims d, const float* __restrict__ V, const float* __restrict__ T, const float* __restrict__ L,
-    const float* __restrict__ theta, const double* __restrict__ Et, const float* __restrict__ XT,
+    const float* __restrict__ theta, const float2* __restrict__ Etab, const float* __restrict__ XT,
     const float* __restrict__ G, uint32_t k0, uint32_t kcount, const uint32_t* __restrict__ flag,
     DevStatus* status, const uint32_t* __restrict__ best_lab, const uint32_t* __restrict__ best_idx,
-    const float* __restrict__ best_lik, unsigned long long* keys)
+    const float* __restrict__ best_lik, unsigned long long* keys, const float* __restrict__ mx)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ ScreenShared sh;
-    typedef cub::BlockReduce<double, kScrThreads> RD;
+    typedef cub::BlockReduce<float, kScrThreads> RF;
     typedef cub::BlockScan<uint32_t, kScrThreads> SC;
     __shared__ union {
-        typename RD::TempStorage rd;
+        typename RF::TempStorage rf;
         typename SC::TempStorage sc;
     } tmp;
     const uint32_t S = d.S, W = d.W, M = d.M, S2 = 2 * S + 1;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kScrThreads / 32;
     uint8_t* fa = smraw;                                            // [S2] bit0 in bounds, bit1 L_f > 0
     uint8_t* pt = fa + ((S2 + 15) & ~15u);                          // [M][S2] L_t > 0
     uint32_t* alist = reinterpret_cast<uint32_t*>(pt + ((M * S2 + 15) & ~15u));  // [S2]
     uint32_t* tb = alist + S2;                                      // [M*S2] (t,b) with L_t > 0
+    float* rowmax = reinterpret_cast<float*>(tb + M * S2);          // [kRowCap]
+    float* vw = rowmax + kRowCap;                                   // [C][W] window voltage
+    float* gmax = vw + d.C * W;                                     // [M] max_b G_t(b) of this window
+    uint32_t* cand = reinterpret_cast<uint32_t*>(gmax + M);         // [kCandCap][3] (a, t, b)
+    __shared__ uint32_t s_ncand;
     const uint64_t items = (uint64_t)S2 * S2 * M;
     const uint64_t nloc = (items - 1) / d.WG + 1;
     const uint64_t slots = nloc * d.WG;
     uint32_t lbits = 0;
     while ((1u << lbits) < d.WG) ++lbits;
-    const double u = 1.0 / 16777216.0;
-    const double K = 1.05 * u * 2.0 * ((double)d.C * W + d.C + W + 8);
+    const float u = 1.0f / 16777216.0f;
+    const float K = 1.01f * 1.05f * u * 2.0f * ((float)d.C * W + d.C + W + 8);
     const uint32_t nflag = status->n_flag;
     unsigned long long exact_n = 0, item_n = 0;
     for (uint32_t kk = blockIdx.x; kk < kcount; kk += gridDim.x) {
@@ -288,15 +329,15 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
         const float seed = best_lik[id];
         const float* Gk = G + (uint64_t)kk * M * S2;
         __syncthreads();
-        // window norm, shift flags, positive-likelihood flags
-        double nv2 = 0.0;
+        float nv2 = 0.f;
         for (uint32_t e = threadIdx.x; e < d.C * W; e += blockDim.x) {
             const uint32_t c = e / W, j = e - c * W;
-            const double v = V[(uint64_t)c * d.N + p + j];
-            nv2 += v * v;
+            const float v = V[(uint64_t)c * d.N + p + j];
+            vw[e] = v;
+            nv2 = fmaf(v, v, nv2);
         }
-        const double nvs = RD(tmp.rd).Sum(nv2);
-        if (threadIdx.x == 0) { sh.nv = sqrt(nvs) * 1.001; sh.best = 0ull; sh.nA = 0; }
+        const float nvs = RF(tmp.rf).Sum(nv2);
+        if (threadIdx.x == 0) { sh.nv = sqrtf(nvs) * 1.001f; sh.best = 0ull; }
         for (uint32_t x = threadIdx.x; x < S2; x += blockDim.x) {
             const uint64_t xp = (uint64_t)x + p;
             const bool inb = xp >= S && xp < (uint64_t)d.N - W + S;
@@ -308,13 +349,23 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
             const bool inb = xp >= S && xp < (uint64_t)d.N - W + S;
             pt[e] = (inb && L[(uint64_t)t * d.N + xp - S] > 0.f) ? 1 : 0;
         }
+        // per-template maxima of the partial correlations over the shifts in bounds
+        for (uint32_t t = warp; t < M; t += nwarps) {
+            float m = -INFINITY;
+            for (uint32_t x = lane; x < S2; x += 32) {
+                const uint64_t xp = (uint64_t)x + p;
+                if (xp >= S && xp < (uint64_t)d.N - W + S) m = fmaxf(m, Gk[(uint64_t)t * S2 + x]);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+            if (lane == 0) gmax[t] = m;
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t n = 0;
             for (uint32_t x = 0; x < S2; ++x) if (fa[x] == 3) alist[n++] = x;
             sh.nA = n;
         }
-        // compact the (t, b) pairs with L_t > 0
         {
             uint32_t base = 0;
             for (uint32_t r0 = 0; r0 < M * S2; r0 += blockDim.x) {
@@ -330,67 +381,13 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
         }
         __syncthreads();
         const uint32_t nA = sh.nA, nTB = sh.nTB;
-        const double nv = sh.nv;
-        // item enumeration: (a in A+, all t, b) then ((t,b) with L_t > 0, a not in A+)
-        auto est_bound = [&](uint32_t a, uint32_t t, uint32_t b, double& est, double& bound) {
-            const double ef = Et[(uint64_t)f * S2 + a], et = Et[(uint64_t)t * S2 + b];
-            est = (double)Gk[(uint64_t)f * S2 + a] + (double)Gk[(uint64_t)t * S2 + b] -
-                  (double)XT[(((uint64_t)f * M + t) * S2 + a) * S2 + b];
-            bound = K * ((sqrt(ef) + sqrt(et)) * nv + ef + et);
-        };
-        const uint64_t n1 = (uint64_t)nA * M * S2;
-        const uint64_t n2 = (uint64_t)nTB * S2;
-        // pass 1: lower bound on the best pair value
-        double lb = -1e300;
-        for (uint64_t i = threadIdx.x; i < n1 + n2; i += blockDim.x) {
-            uint32_t a, t, b;
-            if (i < n1) {
-                b = (uint32_t)(i % S2);
-                const uint64_t r = i / S2;
-                t = (uint32_t)(r % M);
-                a = alist[r / M];
-                if (!(fa[b] & 1) || (a > b ? a - b : b - a) > W) continue;
-            } else {
-                const uint64_t i2 = i - n1;
-                a = (uint32_t)(i2 % S2);
-                const uint32_t e = tb[i2 / S2];
-                t = e / S2;
-                b = e - t * S2;
-                if (fa[a] != 1 || (a > b ? a - b : b - a) > W) continue;
-            }
-            double est, bound;
-            est_bound(a, t, b, est, bound);
-            lb = fmax(lb, est - bound);
-            ++item_n;
-        }
-        const double lbs = RD(tmp.rd).Reduce(lb, cub::Max());
-        if (threadIdx.x == 0) sh.lb = lbs;
-        __syncthreads();
-        const double thr = fmax(fmax(sh.lb, (double)seed), 0.0);
-        // pass 2: exact scores of the items that can reach the threshold
-        unsigned long long kbest = 0ull;
-        for (uint64_t i = threadIdx.x; i < n1 + n2; i += blockDim.x) {
-            uint32_t a, t, b;
-            if (i < n1) {
-                b = (uint32_t)(i % S2);
-                const uint64_t r = i / S2;
-                t = (uint32_t)(r % M);
-                a = alist[r / M];
-                if (!(fa[b] & 1) || (a > b ? a - b : b - a) > W) continue;
-            } else {
-                const uint64_t i2 = i - n1;
-                a = (uint32_t)(i2 % S2);
-                const uint32_t e = tb[i2 / S2];
-                t = e / S2;
-                b = e - t * S2;
-                if (fa[a] != 1 || (a > b ? a - b : b - a) > W) continue;
-            }
-            double est, bound;
-            est_bound(a, t, b, est, bound);
-            if (est + bound < thr) continue;
-            const float v = pair_exact(d, T, V, f, t, p, a, b);
+        const float nv = sh.nv;
+        const uint32_t rows1 = nA * M, rows = rows1 + nTB;
+        const bool keep_rows = rows <= (uint32_t)kRowCap;
+        auto score = [&](uint32_t a, uint32_t t, uint32_t b, unsigned long long& kb) {
+            const float v = pair_exact_sv(d, T, vw, f, t, a, b);
             ++exact_n;
-            if (!(v > 0.f)) continue;
+            if (!(v > 0.f)) return;
             const uint64_t r = (uint64_t)t + (uint64_t)M * a + (uint64_t)M * S2 * b;
             uint32_t pr = item_priority(r, d.WG, lbits);
             for (uint64_t rr = r + items; rr < slots; rr += items) {
@@ -399,14 +396,97 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
             }
             const unsigned long long key =
                 ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - pr);
-            kbest = key > kbest ? key : kbest;
+            kb = key > kb ? key : kb;
+        };
+        // one row: (a fixed, t, lanes over b) or (t, b fixed, lanes over a)
+        auto row_scan = [&](uint32_t row, float thr, bool exact_pass, float& lbm, float& ubm,
+                            unsigned long long& kb) {
+            uint32_t a = 0, t, b = 0;
+            bool fixed_a;
+            if (row < rows1) {
+                a = alist[row / M];
+                t = row % M;
+                fixed_a = true;
+            } else {
+                const uint32_t e = tb[row - rows1];
+                t = e / S2;
+                b = e - t * S2;
+                fixed_a = false;
+            }
+            const float* xt_ft = XT + ((uint64_t)f * M + t) * S2 * S2;
+            if (!exact_pass) {
+                // row bound: every component at least the item's, same float order
+                const float nx = mx[(uint64_t)f * M + t];
+                float ub;
+                if (fixed_a) {
+                    const float2 ea = Etab[(uint64_t)f * S2 + a];
+                    ub = Gk[(uint64_t)f * S2 + a] + gmax[t] + nx +
+                         K * ((ea.y + mx[M * M + t]) * nv + ea.x + mx[M * M + M + t]);
+                } else {
+                    const float2 eb = Etab[(uint64_t)t * S2 + b];
+                    ub = gmax[f] + Gk[(uint64_t)t * S2 + b] + nx +
+                         K * ((mx[M * M + f] + eb.y) * nv + mx[M * M + M + f] + eb.x);
+                }
+                if (ub < thr) { ubm = -INFINITY; return; }
+            }
+            for (uint32_t x = lane; x < S2; x += 32) {
+                if (fixed_a) {
+                    b = x;
+                    if (!(fa[b] & 1)) continue;
+                } else {
+                    a = x;
+                    if (fa[a] != 1) continue;
+                }
+                if ((a > b ? a - b : b - a) > W) continue;
+                const float2 ea = Etab[(uint64_t)f * S2 + a], eb = Etab[(uint64_t)t * S2 + b];
+                const float est = Gk[(uint64_t)f * S2 + a] + Gk[(uint64_t)t * S2 + b] - xt_ft[(uint64_t)a * S2 + b];
+                const float bound = K * ((ea.y + eb.y) * nv + ea.x + eb.x);
+                if (!exact_pass) {
+                    lbm = fmaxf(lbm, est - bound);
+                    ubm = fmaxf(ubm, est + bound);
+                    ++item_n;
+                    continue;
+                }
+                if (est + bound < thr) continue;
+                const uint32_t slot = atomicAdd(&s_ncand, 1u);
+                if (slot < (uint32_t)kCandCap) {
+                    cand[3 * slot] = a;
+                    cand[3 * slot + 1] = t;
+                    cand[3 * slot + 2] = b;
+                } else {
+                    score(a, t, b, kb);   // list full: score in place
+                }
+            }
+        };
+        float lb = -INFINITY;
+        unsigned long long kbest = 0ull;
+        const float thr0 = fmaxf(seed, 0.f);
+        for (uint32_t row = warp; row < rows; row += nwarps) {
+            float lbm = -INFINITY, ubm = -INFINITY;
+            row_scan(row, thr0, false, lbm, ubm, kbest);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) ubm = fmaxf(ubm, __shfl_xor_sync(0xffffffffu, ubm, off));
+            if (keep_rows && lane == 0) rowmax[row] = ubm;
+            lb = fmaxf(lb, lbm);
         }
+        const float lbs = RF(tmp.rf).Reduce(lb, cub::Max());
+        if (threadIdx.x == 0) { sh.lb = lbs; s_ncand = 0; }
+        __syncthreads();
+        const float thr = fmaxf(fmaxf(sh.lb, seed), 0.f);
+        for (uint32_t row = warp; row < rows; row += nwarps) {
+            if (keep_rows && rowmax[row] < thr) continue;
+            float lbm, ubm;
+            row_scan(row, thr, true, lbm, ubm, kbest);
+        }
+        __syncthreads();
+        const uint32_t nc = min(s_ncand, (uint32_t)kCandCap);
+        for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) score(cand[3 * i], cand[3 * i + 1], cand[3 * i + 2], kbest);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             const unsigned long long o = __shfl_down_sync(0xffffffffu, kbest, off);
             kbest = o > kbest ? o : kbest;
         }
-        if ((threadIdx.x & 31) == 0 && kbest) atomicMax(&sh.best, kbest);
+        if (lane == 0 && kbest) atomicMax(&sh.best, kbest);
         __syncthreads();
         if (threadIdx.x == 0 && sh.best) keys[k] = sh.best;
     }
@@ -421,11 +501,12 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     const Layout& L = *w.lay;
     if (!L.screened) return FBP_OK;
     const uint32_t S2 = 2 * d.S + 1;
-    energy_table_kernel<<<(d.M * S2 + 255) / 256, 256, 0, st>>>(d, T, w.at<double>(L.off_et));
+    energy_table_kernel<<<(d.M * S2 + 255) / 256, 256, 0, st>>>(d, T, w.at<float2>(L.off_et));
     const size_t smem = (size_t)2 * d.C * d.W * 4 + 8 + (size_t)kLagChunk * (d.W + 1) * 8;
     if (smem > 200 * 1024) return fail(FBP_E_ARG, "template too large for the pair table kernel");
     FBP_CUDA(cudaFuncSetAttribute(cross_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    cross_table_kernel<<<d.M * d.M, 256, smem, st>>>(d, T, w.at<float>(L.off_xt));
+    cross_table_kernel<<<d.M * d.M, 256, smem, st>>>(d, T, w.at<float>(L.off_xt), w.at<float>(L.off_mx));
+    energy_max_kernel<<<(d.M + 127) / 128, 128, 0, st>>>(d, w.at<float2>(L.off_et), w.at<float>(L.off_mx) + (size_t)d.M * d.M);
     template_order_kernel<<<1, 256, d.M * 4, st>>>(d, T, w.at<uint32_t>(L.off_perm));
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
@@ -447,13 +528,14 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     const size_t smem_a = strip + Q * per_t;
     if (smem_a > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     const size_t smem_b = ((S2 + 15) & ~15u) + (((size_t)d.M * S2 + 15) & ~(size_t)15) + (size_t)S2 * 4 +
-                          (size_t)d.M * S2 * 4;
+                          (size_t)d.M * S2 * 4 + (size_t)kRowCap * 4 + (size_t)d.C * d.W * 4 + (size_t)d.M * 4 +
+                          (size_t)kCandCap * 12;
     if (smem_b > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     FBP_CUDA(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
     const uint32_t threads_a = (S2 + 31) & ~31u;
     const uint32_t groups = (d.M + Q - 1) / Q;
     float* G = w.at<float>(L.off_g);
-    const double* Et = w.at<double>(L.off_et);
+    const float2* Et = w.at<float2>(L.off_et);
     const float* XT = w.at<float>(L.off_xt);
     const uint32_t* perm = w.at<uint32_t>(L.off_perm);
     for (uint32_t k0 = 0; k0 < nflag_max; k0 += (uint32_t)L.gbatch) {
@@ -474,7 +556,8 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
 #undef FBP_PC
         const uint32_t gb = kc < 148u * 8 ? kc : 148u * 8;
         screen_kernel<<<gb, kScrThreads, smem_b, st>>>(d, V, T, w.L(), theta, Et, XT, G, k0, kc, w.flag(), w.status(),
-                                                       w.best_lab(), w.best_idx(), w.best_lik(), w.keys());
+                                                       w.best_lab(), w.best_idx(), w.best_lik(), w.keys(),
+                                                       w.at<float>(L.off_mx));
         FBP_CUDA(cudaGetLastError());
     }
     return FBP_OK;
