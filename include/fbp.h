@@ -125,6 +125,26 @@ int fbp_residual(const fbp_dims* dims, float* voltage, const float* templates,
                  const uint32_t* spike_idx, const uint32_t* spike_lab, uint32_t n,
                  void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free residual subtraction.  No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc at all, such as a plug-in running
+ * inside an acquisition or visualisation host that owns every byte of device
+ * memory and forbids allocation while data stream, so it cannot hand this library
+ * the workspace fbp_residual needs.  Same contract and results as fbp_residual;
+ * the per-spike scratch (window ids, overlap flags, a counter) lives in one
+ * file-scope static device array sized for FBP_NOALLOC_MAX_SPIKES spikes (about
+ * 320 KB), which every GPU that loads the library holds until the process exits.
+ *   - n > FBP_NOALLOC_MAX_SPIKES fails with FBP_E_ARG before any device work.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - Every call shares the one array, which keeps the last call's contents:
+ *     calls whose work overlaps on the GPU (other streams or threads without
+ *     ordering between them) race on it and must be serialised by the caller.
+ * It allocates no device memory and calls no allocating routine. */
+#define FBP_NOALLOC_MAX_SPIKES 65536u
+int fbp_residual_noalloc(const fbp_dims* dims, float* voltage, const float* templates,
+                         const uint32_t* spike_idx, const uint32_t* spike_lab, uint32_t n,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

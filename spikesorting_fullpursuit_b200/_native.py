@@ -25,7 +25,8 @@ FBP_TIMING = 0x4
 
 # every function include/fbp.h declares
 EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_pursue_chunk",
-           "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual")
+           "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc")
+NOALLOC_MAX_SPIKES = 65536
 
 
 class FbpDims(ctypes.Structure):
@@ -77,6 +78,8 @@ def lib():
     L.fbp_likelihood.restype = ctypes.c_int
     L.fbp_residual.argtypes = [P(FbpDims), vp, vp, vp, vp, u32, vp, sz, vp]
     L.fbp_residual.restype = ctypes.c_int
+    L.fbp_residual_noalloc.argtypes = [P(FbpDims), vp, vp, vp, vp, u32, vp]
+    L.fbp_residual_noalloc.restype = ctypes.c_int
     _lib = L
     return L
 
