@@ -280,27 +280,35 @@ def main():
                  "stages_ms": {k: v for k, v in st_plain.items() if k.startswith("ms_")}}
 
     hbm, tflops, peak_kind = load_peaks()
-    # dominant stage and its roofline
-    stages = {k[3:]: v for k, v in st_stage.items() if k.startswith("ms_") and k != "ms_total"}
-    dom = max(stages, key=stages.get)
-    listed = st_stage["listed"]
-    lik_flop = 2.0 * M * C * W * W * listed
-    if dom == "likelihood":
-        achieved = lik_flop / (stages[dom] * 1e-3) / 1e12
-        roof = {"kernel": "likelihood", "bound": "tensor", "achieved": achieved, "peak": tflops,
-                "unit": "TFLOP/s", "frac": achieved / tflops, "traffic": None,
-                "peak_kind": peak_kind}
-    elif dom == "overlap":
-        flagged = st_stage["flagged"]
-        flop = 2.0 * C * W * M * (2 * S + 1) * flagged
-        achieved = flop / (stages[dom] * 1e-3) / 1e12
-        roof = {"kernel": "overlap_recheck", "bound": "tensor", "achieved": achieved, "peak": tflops,
-                "unit": "TFLOP/s", "frac": achieved / tflops, "traffic": None, "peak_kind": peak_kind}
-    else:
-        byts = 4.0 * M * N * 3 + 12.0 * N / W
-        achieved = byts / (stages[dom] * 1e-3) / 1e9
-        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind}
+    # per-kernel device time of one step (separate run with FBP_TIMING) and the
+    # algorithmic work each kernel family does in that step
+    S2 = 2 * S + 1
+    listed, flagged = st_stage["listed"], st_stage["flagged"]
+    fam = {
+        "lik_tc_kernel": (st_stage["ms_lik_tc"], "tensor", 2.0 * M * C * W * W * listed),
+        "fixup_kernel": (st_stage["ms_fixup"], "fp32", 2.0 * C * W * st_stage["fixups"]),
+        "partial_corr_kernel": (st_stage["ms_partial_corr"], "fp32", 2.0 * M * C * W * S2 * flagged),
+        "screen_kernel": (st_stage["ms_screen"], "hbm", (4.0 * C * W + 8.0 * M * S2 + 4.0 * M * S2) * flagged),
+        "score_kernel": (st_stage["ms_score"], "fp32", 5.0 * C * W * st_stage["pair_exact"]),
+        "argmax_kernel": (st_stage["ms_argmax"], "hbm", 12.0 * M * W * listed + 22.0 * listed),
+    }
+    kernels = {}
+    for name, (ms, bound, work) in fam.items():
+        if ms <= 0:
+            continue
+        if bound == "hbm":
+            ach = work / (ms * 1e-3) / 1e9
+            kernels[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                             "frac": ach / hbm}
+        else:
+            ach = work / (ms * 1e-3) / 1e12
+            kernels[name] = {"ms": ms, "bound": "tensor" if bound == "tensor" else "fp32-simt",
+                             "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops}
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    roof = dict(kernels[dom])
+    roof.update({"kernel": dom, "traffic": None, "peak_kind": peak_kind,
+                 "note": "peak = measured dense bf16 (TF32 nominal is half of it); hbm = measured copy"})
+    launches = int(st_fast["launches"]) * args.steps
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -320,8 +328,9 @@ def main():
                        "spikes": n_sp, "passes": st_fast["passes"], "mode": "fast"},
             "e2e": {"value": e2e_value, "unit": "Msample*ch/s", "h2d_bytes_per_step": int(4 * C * N + T.nbytes + 8 * M),
                     "d2h_bytes_per_step": int(8 * n_sp), "ms_per_step": e2e_t / len(e2e_ms)},
-            "gpu_launches": None,
-            "stages_ms": stages,
+            "gpu_launches": launches,
+            "stages_ms": {k[3:]: v for k, v in st_stage.items() if k.startswith("ms_") and v > 0},
+            "kernels": kernels,
             "stats": {k: st_stage[k] for k in ("passes", "n_spikes", "listed", "flagged", "fixups", "pair_exact")},
             "roofline": roof,
             "plain_fp32": plain,

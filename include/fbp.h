@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define FBP_ABI_VERSION 1
+#define FBP_ABI_VERSION 2
 
 typedef enum fbp_status {
     FBP_OK = 0,
@@ -64,7 +64,21 @@ typedef struct fbp_chunk_stats {
     float ms_accept;
     float ms_residual;
     float ms_total;
+    /* device time per kernel family, summed over passes (0 unless timing) */
+    float ms_lik_tc;         /* tensor-core likelihood */
+    float ms_fixup;          /* exact recomputation of queued likelihood samples */
+    float ms_lik_exact;      /* plain FP32 likelihood */
+    float ms_partial_corr;   /* partial correlations of the screened recheck */
+    float ms_screen;         /* screening of the recheck items */
+    float ms_score;          /* exact scoring of the recheck candidates */
+    float ms_overlap_plain;  /* brute-force recheck */
+    uint32_t pad0;
+    uint64_t launches;       /* kernels launched by the call */
 } fbp_chunk_stats;
+
+/* Option bit: record per-stage and per-kernel device times in the stats
+ * (serialises the stream around each timed launch; for profiling). */
+#define FBP_TIMING 0x4u
 
 /* Library ABI version (FBP_ABI_VERSION). */
 int fbp_abi_version(void);

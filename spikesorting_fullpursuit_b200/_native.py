@@ -41,7 +41,12 @@ class FbpChunkStats(ctypes.Structure):
                 ("fixups", ctypes.c_uint64), ("pair_exact", ctypes.c_uint64),
                 ("ms_likelihood", ctypes.c_float), ("ms_argmax", ctypes.c_float),
                 ("ms_overlap", ctypes.c_float), ("ms_accept", ctypes.c_float),
-                ("ms_residual", ctypes.c_float), ("ms_total", ctypes.c_float)]
+                ("ms_residual", ctypes.c_float), ("ms_total", ctypes.c_float),
+                ("ms_lik_tc", ctypes.c_float), ("ms_fixup", ctypes.c_float),
+                ("ms_lik_exact", ctypes.c_float), ("ms_partial_corr", ctypes.c_float),
+                ("ms_screen", ctypes.c_float), ("ms_score", ctypes.c_float),
+                ("ms_overlap_plain", ctypes.c_float), ("pad0", ctypes.c_uint32),
+                ("launches", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -27,6 +27,34 @@ int fail(int status, const std::string& msg)
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+KernelClock& kclock()
+{
+    static thread_local KernelClock c;
+    return c;
+}
+
+KScope::KScope(float fbp_chunk_stats::*field, cudaStream_t st) : st_(st)
+{
+    KernelClock& c = kclock();
+    if (!c.stats) return;
+    acc_ = &(c.stats->*field);
+    cudaEventCreate(&ev_[0]);
+    cudaEventCreate(&ev_[1]);
+    cudaEventRecord(ev_[0], st_);
+}
+
+KScope::~KScope()
+{
+    if (!acc_) return;
+    cudaEventRecord(ev_[1], st_);
+    cudaEventSynchronize(ev_[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+    *acc_ += ms;
+    cudaEventDestroy(ev_[0]);
+    cudaEventDestroy(ev_[1]);
+}
+
 bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
 {
     if (!d || !L) return false;
@@ -99,8 +127,10 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
             if (gb > L->nw) gb = L->nw;
             L->gbatch = gb;
             L->off_g = take(gb * per);
-            L->off_perm = take(M * 4);
+            L->off_perm = take(M * 4 + 8 + M * 8);      // order, then (8-aligned) non-zero channel masks
             L->off_mx = take(M * M * 4 + 2 * M * 4);   // max -X_ft per pair; max sqrt(E), max E per template
+            L->cand_cap = 16ull << 20;                  // exact-scoring candidates per batch
+            L->off_cand = take(L->cand_cap * 8);
         }
     }
     L->bytes = align_up(off, 256);
@@ -182,6 +212,11 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     fbp_chunk_stats local{};
     fbp_chunk_stats& S = stats ? *stats : local;
     std::memset(&S, 0, sizeof(S));
+    kclock().stats = timing ? &S : nullptr;
+    kclock().launches = 0;
+    struct ClockReset {
+        ~ClockReset() { kclock().stats = nullptr; }
+    } clock_reset;
     Layout cur = lay;
     Work w{&cur, static_cast<unsigned char*>(workspace)};
     const Dims d = dims_of(lay);
@@ -264,6 +299,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     FBP_CUDA(cudaStreamSynchronize(st));
     S.pair_exact = (plain || !lay.screened) ? hs.pair_items : hs.n_pair_exact;
     S.n_spikes = total;
+    S.launches = kclock().launches;
     *n_spikes = total;
     return FBP_OK;
 }

@@ -25,6 +25,30 @@ int fail(int status, const std::string& msg);
     } while (0)
 
 // ---------------------------------------------------------------------------
+// Per-call instrumentation: kernel launch counts, and (with FBP_TIMING) device
+// time per kernel family.  Thread-local; set up by the C-ABI entry points.
+// ---------------------------------------------------------------------------
+struct KernelClock {
+    fbp_chunk_stats* stats = nullptr;  // non-null: time the launches
+    uint64_t launches = 0;
+};
+KernelClock& kclock();
+
+inline void count_launch(uint32_t n = 1) { kclock().launches += n; }
+
+// Times the launches issued in its scope into *acc (if timing is on).
+class KScope {
+  public:
+    KScope(float fbp_chunk_stats::*field, cudaStream_t st);
+    ~KScope();
+
+  private:
+    float* acc_ = nullptr;
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
+    cudaStream_t st_ = nullptr;
+};
+
+// ---------------------------------------------------------------------------
 // Device status word: counters the kernels of one pass publish.
 // ---------------------------------------------------------------------------
 struct DevStatus {
@@ -37,6 +61,8 @@ struct DevStatus {
     uint32_t n_pair_exact;  // overlap items recomputed exactly
     uint32_t n_conf;        // spikes of this pass overlapping an earlier one
     unsigned long long pair_items;  // items evaluated by the overlap recheck
+    uint32_t cand_count;    // candidates appended to the exact-scoring list (per batch)
+    uint32_t pad2;
 };
 
 // ---------------------------------------------------------------------------
@@ -54,7 +80,8 @@ struct Layout {
     // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
     // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
     // template processing order perm[M]
-    size_t off_et, off_xt, off_g, off_perm, off_mx;
+    size_t off_et, off_xt, off_g, off_perm, off_mx, off_cand;
+    uint64_t cand_cap;
     uint64_t gbatch;
     bool screened;
     size_t bytes;

@@ -254,6 +254,7 @@ int compact(F f, const uint32_t* n_dev, uint32_t n_upper, uint32_t* blk, uint32_
         FBP_CUDA(cudaMemsetAsync(total, 0, sizeof(uint32_t), st));
         return FBP_OK;
     }
+    count_launch(3);
     compact_count<F><<<nb, kCompactThreads, 0, st>>>(f, n_dev, n_upper, blk);
     compact_scan<<<1, 1024, 0, st>>>(blk, nb, total);
     compact_scatter<F><<<nb, kCompactThreads, 0, st>>>(f, n_dev, n_upper, blk);
@@ -849,6 +850,7 @@ inline uint32_t grid_for(uint64_t n, uint32_t threads, uint32_t cap = 148 * 32)
 
 int launch_iota(uint32_t* list, uint32_t n, cudaStream_t st)
 {
+    count_launch();
     iota_kernel<<<grid_for(n, 256), 256, 0, st>>>(list, n);
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
@@ -873,6 +875,8 @@ int launch_likelihood_exact(const Dims& d, const float* V, const float* T, const
         FBP_CUDA(cudaFuncSetAttribute(lik_exact_kernel<QQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
         lik_exact_kernel<QQ><<<grid, threads, smem, st>>>(d, V, T, bias, list, nlist, L);       \
         break;
+    count_launch();
+    KScope ks(&fbp_chunk_stats::ms_lik_exact, st);
     switch (Q) {
         FBP_LIK(8)
         FBP_LIK(4)
@@ -889,6 +893,7 @@ int launch_argmax(const Dims& d, const Work& w, const uint32_t* list, uint32_t n
     if (nlist == 0) return FBP_OK;
     const uint32_t threads = 256;
     const uint64_t warps = nlist;
+    count_launch();
     argmax_kernel<<<grid_for(warps * 32, threads, 148 * 64), threads, 0, st>>>(
         d, w.L(), list, nlist, w.best_lik(), w.best_lab(), w.best_idx(), w.check(), w.orech(),
         w.ov_idx(), w.ov_lab());
@@ -917,6 +922,8 @@ int launch_overlap_plain(const Dims& d, const Work& w, const float* V, const flo
     FBP_CUDA(cudaMemsetAsync(w.keys(), 0, sizeof(unsigned long long) * nflag_max, st));
     const uint64_t tasks = (uint64_t)nflag_max * d.M;
     const uint32_t grid = (uint32_t)(tasks < 148ull * 8 ? tasks : 148ull * 8);
+    count_launch();
+    KScope ks(&fbp_chunk_stats::ms_overlap_plain, st);
     overlap_plain_kernel<<<grid, kOvThreads, smem, st>>>(d, V, T, w.L(), theta, w.flag(), w.status(),
                                                          w.best_lab(), w.best_idx(), w.keys(),
                                                          &w.status()->pair_items);
@@ -928,6 +935,7 @@ int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint
 {
     if (nflag_max == 0) return FBP_OK;
     const uint32_t g = grid_for(nflag_max, 256);
+    count_launch(5);
     parse_kernel<<<g, 256, 0, st>>>(d, w.L(), theta, w.flag(), w.status(), w.keys(), w.best_lik(),
                                     w.best_lab(), w.best_idx(), w.orech(), w.ov_idx(), w.ov_lab());
     reassign_resolve_kernel<<<g, 256, 0, st>>>(d, w.flag(), w.status(), w.orech(), w.ov_idx(), w.orech_fin());
@@ -947,6 +955,7 @@ int launch_accept(const Dims& d, const Work& w, const float* theta, uint32_t nli
         return FBP_OK;
     }
     const uint32_t g = grid_for(nlist, 256);
+    count_launch(4);
     accept_decide_kernel<<<g, 256, 0, st>>>(d, w.list(), nlist, theta, w.best_lik(), w.best_lab(),
                                             w.best_idx(), w.orech(), w.has());
     AcceptCtx cx{d, w.list(), nlist, w.has(), w.check(), w.best_lik(), w.best_lab(), w.best_idx(), theta};
@@ -970,6 +979,7 @@ int launch_residual(const Dims& d, const Work& w, float* V, const float* T, cons
     if (n == 0) return FBP_OK;
     const uint32_t back = 4 + 2 * ((d.S + d.W - 1) / d.W);
     FBP_CUDA(cudaMemsetAsync(&w.status()->n_conf, 0, 4, st));
+    count_launch(2);
     residual_parallel_kernel<<<n, 128, 0, st>>>(d, V, T, idx, lab, win, n, back, w.pconf(), &w.status()->n_conf);
     residual_ordered_kernel<<<1, 1024, 0, st>>>(d, V, T, idx, lab, n, w.pconf(), &w.status()->n_conf);
     FBP_CUDA(cudaGetLastError());
@@ -980,6 +990,7 @@ int launch_adjusted_clips(const Dims& d, const float* V, const float* T, const u
                           const uint32_t* lab, uint32_t n, float* clips, cudaStream_t st)
 {
     if (n == 0) return FBP_OK;
+    count_launch();
     clips_kernel<<<n < 65535u * 4 ? n : 65535u * 4, 128, 0, st>>>(d, V, T, idx, lab, n, clips);
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;

@@ -445,6 +445,7 @@ int launch_tc_prepare_templates(const Dims& d, const Work& w, const float* T, cu
     TcConfig c;
     if (!tc_config(d, &c)) return FBP_OK;
     const Layout& L = *w.lay;
+    count_launch();
     template_pack_kernel<<<256, 256, 0, st>>>(d, T, c.Cq, c.Np, w.at<float>(L.off_tt_hi), w.at<float>(L.off_tnorm));
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
@@ -458,6 +459,7 @@ int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const
     if (!tc_config(d, &c)) return FBP_OK;
     const Layout& L = *w.lay;
     float4* Vq = w.at<float4>(L.off_vt_hi);
+    count_launch();
     if (all) {
         voltage_pack_kernel<<<148 * 16, 256, 0, st>>>(d, V, c.Cq, (uint32_t)L.vq_rows, Vq);
     } else if (n > 0) {
@@ -509,7 +511,12 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     FBP_CUDA(cudaMemsetAsync(&w.status()->n_fix, 0, 4, st));
     FBP_CUDA(cudaFuncSetAttribute(lik_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
     const uint32_t grid = (uint32_t)((items + c.ntiles - 1) / c.ntiles);
-    lik_tc_kernel<<<grid, kThreads, c.smem, st>>>(P);
+    count_launch(2);
+    {
+        KScope ks(&fbp_chunk_stats::ms_lik_tc, st);
+        lik_tc_kernel<<<grid, kThreads, c.smem, st>>>(P);
+    }
+    KScope ks(&fbp_chunk_stats::ms_fixup, st);
     fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, bias, P.fix, P.fix_cap, w.status(), Lk);
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;

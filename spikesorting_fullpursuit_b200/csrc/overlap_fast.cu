@@ -117,15 +117,23 @@ __global__ void energy_max_kernel(Dims d, const float2* __restrict__ Et, float* 
 
 // Template processing order for the partial correlations: sorted by the
 // first non-zero channel so groups of neighbouring templates share channels.
-__global__ void template_order_kernel(Dims d, const float* __restrict__ T, uint32_t* perm)
+__global__ void template_order_kernel(Dims d, const float* __restrict__ T, uint32_t* perm,
+                                      unsigned long long* chmask)
 {
     extern __shared__ uint32_t key[];
     for (uint32_t t = threadIdx.x; t < d.M; t += blockDim.x) {
         uint32_t first = d.C;
-        for (uint32_t c = 0; c < d.C && first == d.C; ++c)
-            for (uint32_t j = 0; j < d.W; ++j)
-                if (T[((uint64_t)t * d.C + c) * d.W + j] != 0.f) { first = c; break; }
+        unsigned long long m = 0ull;
+        for (uint32_t c = 0; c < d.C; ++c) {
+            bool nz = false;
+            for (uint32_t j = 0; j < d.W && !nz; ++j) nz = T[((uint64_t)t * d.C + c) * d.W + j] != 0.f;
+            if (nz) {
+                if (first == d.C) first = c;
+                m |= c < 64 ? (1ull << c) : 0ull;
+            }
+        }
         key[t] = first;
+        chmask[t] = d.C <= 64 ? m : ~0ull;   // more than 64 channels: no skipping
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -155,6 +163,7 @@ __global__ void __launch_bounds__(1024) partial_corr_kernel(Dims d, const float*
                                                             const float* __restrict__ theta,
                                                             const float2* __restrict__ Et,
                                                             const uint32_t* __restrict__ perm,
+                                                            const unsigned long long* __restrict__ chmask,
                                                             const uint32_t* __restrict__ flag,
                                                             const DevStatus* status,
                                                             const uint32_t* __restrict__ best_lab,
@@ -185,14 +194,15 @@ __global__ void __launch_bounds__(1024) partial_corr_kernel(Dims d, const float*
         const uint32_t gi = g0 + q;
         Ts[e] = (gi < d.M && j < W) ? T[((uint64_t)perm[gi] * C + c) * W + j] : 0.f;
     }
-    if (threadIdx.x == 0) nch = 0;
-    __syncthreads();
-    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) {
-        bool nz = false;
-        for (uint32_t q = 0; q < Q && !nz; ++q)
-            for (uint32_t j = 0; j < W; ++j)
-                if (Ts[q * tq + c * Wp + j] != 0.f) { nz = true; break; }
-        if (nz) chans[atomicAdd(&nch, 1u)] = c;  // order is irrelevant for an estimate
+    if (threadIdx.x == 0) {
+        // channels where any template of the group is non-zero (order irrelevant for an estimate)
+        unsigned long long m = 0ull;
+        for (uint32_t q = 0; q < Q; ++q)
+            if (g0 + q < d.M) m |= chmask[perm[g0 + q]];
+        uint32_t n = 0;
+        for (uint32_t c = 0; c < C; ++c)
+            if (c >= 64 || ((m >> c) & 1ull)) chans[n++] = c;
+        nch = n;
     }
     __syncthreads();
     const uint32_t b = threadIdx.x;
@@ -234,26 +244,25 @@ __global__ void __launch_bounds__(1024) partial_corr_kernel(Dims d, const float*
 }
 
 // Exact pair likelihood in the reference's float order (binary_pursuit.cl:578-632),
-// with the window's voltage vw[C][W] in shared memory.
-__device__ float pair_exact_sv(const Dims& d, const float* __restrict__ T, const float* vw, uint32_t f, uint32_t t,
-                               uint32_t a, uint32_t b)
+// operands read from memory.
+__device__ float pair_exact_g(const Dims& d, const float* __restrict__ T, const float* __restrict__ V, uint32_t f,
+                              uint32_t t, uint32_t p, uint32_t a, uint32_t b)
 {
     const int W = (int)d.W, fa = (int)d.S - (int)a, ta = (int)d.S - (int)b;
-    const int jlo_f = max(0, -fa), jhi_f = min(W, W - fa);
-    const int jlo_t = max(0, -ta), jhi_t = min(W, W - ta);
+    const int jlo_f = max(0, -fa), jhi_f = min(W, W - fa), jlo_t = max(0, -ta), jhi_t = min(W, W - ta);
     float acc = 0.f;
     for (uint32_t c = 0; c < d.C; ++c) {
         const float* fr = T + ((uint64_t)f * d.C + c) * d.W + fa;
         const float* tr = T + ((uint64_t)t * d.C + c) * d.W + ta;
-        const float* vr = vw + c * d.W;
+        const float* vr = V + (uint64_t)c * d.N + p;
         float ss = 0.f;
-#pragma unroll 4
+#pragma unroll 8
         for (int j = 0; j < W; ++j) {
             const float fv = (j >= jlo_f && j < jhi_f) ? __ldg(fr + j) : 0.f;
             const float tv = (j >= jlo_t && j < jhi_t) ? __ldg(tr + j) : 0.f;
-            const float s = fadd(fv, tv);
-            ss = fadd(ss, fmul(s, s));
-            acc = fadd(acc, fmul(s, vr[j]));
+            const float sv = fadd(fv, tv);
+            ss = fadd(ss, fmul(sv, sv));
+            acc = fadd(acc, fmul(sv, __ldg(vr + j)));
         }
         if (ss > 0.f) acc = fsub(acc, fmul(0.5f, ss));
     }
@@ -268,32 +277,40 @@ __device__ __forceinline__ uint32_t item_priority(uint64_t r, uint32_t WG, uint3
 }
 
 constexpr int kScrThreads = 256;
-constexpr int kRowCap = 8192;   // per-row upper bounds kept in shared memory
-constexpr int kCandCap = 2048;  // exact-scoring candidates per window pass
+constexpr int kRowCap = 2048;   // surviving rows kept in shared memory
+constexpr int kCandCap = 1024;  // exact-scoring candidates per window
+constexpr int kRowUnroll = 8;   // items per lane whose loads are in flight together
+constexpr uint32_t kGStage = 48 * 1024;  // partial-correlation table staged in shared memory up to this size
 
 struct ScreenShared {
     float lb;
     float nv;
     unsigned long long best;
     uint32_t nA;
-    uint32_t nTB;
+    uint32_t nrows;
+    uint32_t ncand;
+    uint32_t gfull;   // the global candidate list ran out of room for this window
 };
 
-// Screening of one flagged window per CTA.  Items are enumerated as rows:
-// part 1 = (a in A+, t) rows over all b; part 2 = ((t, b) with L_t > 0) rows
-// over the a not in A+.  A warp handles a row, lanes the varying shift.
-// Pass 1 gives the lower bound LB = max(est - bound) and per-row maxima of
-// est + bound; pass 2 revisits only rows that can reach max(LB, seed) and
-// scores their candidates exactly.
+// Screening of one flagged window per CTA.
+//   rows, part 1: (a in A+, t) -- fixed a, the warp's lanes run over b;
+//   rows, part 2: (t, b) with L_t(b) > 0 -- fixed b, lanes run over a not in A+.
+// Phase B bounds every row from shared-memory quantities (each component at least
+// the item's, same monotone float order) and keeps the rows that can reach the
+// window's seed.  Phase C scans the kept rows: LB = max(est - bound) and per-row
+// maxima of est + bound.  Phase D lists the items of rows reaching max(LB, seed)
+// whose interval does; phase E scores them exactly, in parallel.
 __global__ void __launch_bounds__(kScrThreads) screen_kernel(
     Dims d, const float* __restrict__ V, const float* __restrict__ T, const float* __restrict__ L,
     const float* __restrict__ theta, const float2* __restrict__ Etab, const float* __restrict__ XT,
     const float* __restrict__ G, uint32_t k0, uint32_t kcount, const uint32_t* __restrict__ flag,
     DevStatus* status, const uint32_t* __restrict__ best_lab, const uint32_t* __restrict__ best_idx,
-    const float* __restrict__ best_lik, unsigned long long* keys, const float* __restrict__ mx)
+    const float* __restrict__ best_lik, unsigned long long* keys, const float* __restrict__ mx,
+    unsigned long long* gcand, uint32_t gcand_cap, const unsigned long long* __restrict__ chmask)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ ScreenShared sh;
+    __shared__ uint32_t s_gbase;
     typedef cub::BlockReduce<float, kScrThreads> RF;
     typedef cub::BlockScan<uint32_t, kScrThreads> SC;
     __shared__ union {
@@ -302,15 +319,24 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
     } tmp;
     const uint32_t S = d.S, W = d.W, M = d.M, S2 = 2 * S + 1;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kScrThreads / 32;
-    uint8_t* fa = smraw;                                            // [S2] bit0 in bounds, bit1 L_f > 0
-    uint8_t* pt = fa + ((S2 + 15) & ~15u);                          // [M][S2] L_t > 0
-    uint32_t* alist = reinterpret_cast<uint32_t*>(pt + ((M * S2 + 15) & ~15u));  // [S2]
-    uint32_t* tb = alist + S2;                                      // [M*S2] (t,b) with L_t > 0
-    float* rowmax = reinterpret_cast<float*>(tb + M * S2);          // [kRowCap]
-    float* vw = rowmax + kRowCap;                                   // [C][W] window voltage
-    float* gmax = vw + d.C * W;                                     // [M] max_b G_t(b) of this window
-    uint32_t* cand = reinterpret_cast<uint32_t*>(gmax + M);         // [kCandCap][3] (a, t, b)
-    __shared__ uint32_t s_ncand;
+    // shared layout
+    float* gf = reinterpret_cast<float*>(smraw);          // [S2]   G_f(a)
+    float2* eft = reinterpret_cast<float2*>(gf + ((S2 + 3) & ~3u));  // [S2] (E_f(a), sqrt)
+    float* gmax = reinterpret_cast<float*>(eft + S2);     // [M] max_b G_t(b) in bounds
+    float* nx = gmax + M;                                  // [M] max -X_ft over items
+    float* ms = nx + M;                                    // [M] max_b sqrt(E_t(b))
+    float* me = ms + M;                                    // [M] max_b E_t(b)
+    float* vw = me + M;                                    // [C][W] window voltage
+    float* rowmax = vw + d.C * W;                          // [kRowCap]
+    uint32_t* rows = reinterpret_cast<uint32_t*>(rowmax + kRowCap);  // [kRowCap]
+    uint32_t* cand = rows + kRowCap;                       // [kCandCap][3]
+    uint32_t* alist = cand + 3 * kCandCap;                 // [S2]
+    uint8_t* fa = reinterpret_cast<uint8_t*>(alist + S2);  // [S2] bit0 in bounds, bit1 L_f > 0
+    uint8_t* pt = fa + ((S2 + 15) & ~15u);                 // [M][S2] L_t > 0
+    // [M][S2] staged G (if it fits), 16-byte aligned for vector stores
+    float* gst = reinterpret_cast<float*>(
+        smraw + ((static_cast<size_t>(pt + ((M * S2 + 15) & ~15u) - smraw) + 15) & ~static_cast<size_t>(15)));
+    const bool gstaged = (uint64_t)M * S2 * 4 <= kGStage;
     const uint64_t items = (uint64_t)S2 * S2 * M;
     const uint64_t nloc = (items - 1) / d.WG + 1;
     const uint64_t slots = nloc * d.WG;
@@ -327,8 +353,10 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
         const uint32_t f = best_lab[id], p = best_idx[id];
         if (window_skipped(d, L, theta, f, p)) continue;
         const float seed = best_lik[id];
+        const float thr0 = fmaxf(seed, 0.f);
         const float* Gk = G + (uint64_t)kk * M * S2;
         __syncthreads();
+        // ---- phase A: window quantities
         float nv2 = 0.f;
         for (uint32_t e = threadIdx.x; e < d.C * W; e += blockDim.x) {
             const uint32_t c = e / W, j = e - c * W;
@@ -336,20 +364,36 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
             vw[e] = v;
             nv2 = fmaf(v, v, nv2);
         }
-        const float nvs = RF(tmp.rf).Sum(nv2);
-        if (threadIdx.x == 0) { sh.nv = sqrtf(nvs) * 1.001f; sh.best = 0ull; }
         for (uint32_t x = threadIdx.x; x < S2; x += blockDim.x) {
             const uint64_t xp = (uint64_t)x + p;
             const bool inb = xp >= S && xp < (uint64_t)d.N - W + S;
             fa[x] = inb ? ((L[(uint64_t)f * d.N + xp - S] > 0.f) ? 3 : 1) : 0;
+            gf[x] = Gk[(uint64_t)f * S2 + x];
+            eft[x] = Etab[(uint64_t)f * S2 + x];
         }
+        if (gstaged) {
+            if (((M * S2) & 3u) == 0 && ((reinterpret_cast<uintptr_t>(Gk) & 15u) == 0)) {
+                const float4* g4 = reinterpret_cast<const float4*>(Gk);
+                float4* s4 = reinterpret_cast<float4*>(gst);
+#pragma unroll 4
+                for (uint32_t e = threadIdx.x; e < M * S2 / 4; e += blockDim.x) s4[e] = g4[e];
+            } else {
+#pragma unroll 8
+                for (uint32_t e = threadIdx.x; e < M * S2; e += blockDim.x) gst[e] = Gk[e];
+            }
+        }
+#pragma unroll 8
         for (uint32_t e = threadIdx.x; e < M * S2; e += blockDim.x) {
             const uint32_t t = e / S2, x = e - t * S2;
             const uint64_t xp = (uint64_t)x + p;
             const bool inb = xp >= S && xp < (uint64_t)d.N - W + S;
             pt[e] = (inb && L[(uint64_t)t * d.N + xp - S] > 0.f) ? 1 : 0;
         }
-        // per-template maxima of the partial correlations over the shifts in bounds
+        for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
+            nx[t] = mx[(uint64_t)f * M + t];
+            ms[t] = mx[(uint64_t)M * M + t];
+            me[t] = mx[(uint64_t)M * M + M + t];
+        }
         for (uint32_t t = warp; t < M; t += nwarps) {
             float m = -INFINITY;
             for (uint32_t x = lane; x < S2; x += 32) {
@@ -360,127 +404,228 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
             for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
             if (lane == 0) gmax[t] = m;
         }
+        const float nvs = RF(tmp.rf).Sum(nv2);
+        if (threadIdx.x == 0) { sh.nv = sqrtf(nvs) * 1.001f; sh.best = 0ull; sh.nrows = 0; sh.ncand = 0; sh.gfull = 0; }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t n = 0;
-            for (uint32_t x = 0; x < S2; ++x) if (fa[x] == 3) alist[n++] = x;
-            sh.nA = n;
-        }
+        // A+ list in ascending order
         {
             uint32_t base = 0;
-            for (uint32_t r0 = 0; r0 < M * S2; r0 += blockDim.x) {
-                const uint32_t e = r0 + threadIdx.x;
-                const uint32_t fl = (e < M * S2 && pt[e]) ? 1u : 0u;
+            for (uint32_t x0 = 0; x0 < S2; x0 += blockDim.x) {
+                const uint32_t x = x0 + threadIdx.x;
+                const uint32_t fl = (x < S2 && fa[x] == 3) ? 1u : 0u;
                 uint32_t off, tot;
                 SC(tmp.sc).ExclusiveSum(fl, off, tot);
-                if (fl) tb[base + off] = e;
+                if (fl) alist[base + off] = x;
                 base += tot;
                 __syncthreads();
             }
-            if (threadIdx.x == 0) sh.nTB = base;
+            if (threadIdx.x == 0) sh.nA = base;
         }
         __syncthreads();
-        const uint32_t nA = sh.nA, nTB = sh.nTB;
+        const uint32_t nA = sh.nA;
         const float nv = sh.nv;
-        const uint32_t rows1 = nA * M, rows = rows1 + nTB;
-        const bool keep_rows = rows <= (uint32_t)kRowCap;
-        auto score = [&](uint32_t a, uint32_t t, uint32_t b, unsigned long long& kb) {
-            const float v = pair_exact_sv(d, T, vw, f, t, a, b);
-            ++exact_n;
-            if (!(v > 0.f)) return;
-            const uint64_t r = (uint64_t)t + (uint64_t)M * a + (uint64_t)M * S2 * b;
-            uint32_t pr = item_priority(r, d.WG, lbits);
-            for (uint64_t rr = r + items; rr < slots; rr += items) {
-                const uint32_t p2 = item_priority(rr, d.WG, lbits);
-                pr = p2 < pr ? p2 : pr;
+        const uint32_t rows1 = nA * M, rows_all = rows1 + M * S2;
+        // ---- phase B: row bounds, keep rows that can reach the seed
+        bool overflow = false;
+        for (uint32_t r = threadIdx.x; r < rows_all; r += blockDim.x) {
+            float ub;
+            if (r < rows1) {
+                const uint32_t a = alist[r / M], t = r % M;
+                const float2 ea = eft[a];
+                ub = gf[a] + gmax[t] + nx[t] + K * ((ea.y + ms[t]) * nv + ea.x + me[t]);
+            } else {
+                const uint32_t e = r - rows1;
+                if (!pt[e]) continue;
+                const uint32_t t = e / S2, b = e - t * S2;
+                const float2 eb = Etab[(uint64_t)t * S2 + b];
+                ub = gmax[f] + Gk[(uint64_t)t * S2 + b] + nx[t] + K * ((ms[f] + eb.y) * nv + me[f] + eb.x);
             }
-            const unsigned long long key =
-                ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - pr);
-            kb = key > kb ? key : kb;
-        };
-        // one row: (a fixed, t, lanes over b) or (t, b fixed, lanes over a)
-        auto row_scan = [&](uint32_t row, float thr, bool exact_pass, float& lbm, float& ubm,
-                            unsigned long long& kb) {
-            uint32_t a = 0, t, b = 0;
+            if (ub < thr0) continue;
+            const uint32_t slot = atomicAdd(&sh.nrows, 1u);
+            if (slot < (uint32_t)kRowCap) { rows[slot] = r; rowmax[slot] = ub; }
+        }
+        __syncthreads();
+        uint32_t nrows = sh.nrows;
+        if (nrows > (uint32_t)kRowCap) { overflow = true; nrows = rows_all; }
+        // row scan: (a fixed, lanes over b) or (t, b fixed, lanes over a); every
+        // load of the lane's items is issued before any arithmetic
+        auto row_items = [&](uint32_t r, float thr, bool listing, float& lbm, float& ubm) {
+            uint32_t a0 = 0, t, b0 = 0;
             bool fixed_a;
-            if (row < rows1) {
-                a = alist[row / M];
-                t = row % M;
+            if (r < rows1) {
+                a0 = alist[r / M];
+                t = r % M;
                 fixed_a = true;
             } else {
-                const uint32_t e = tb[row - rows1];
+                const uint32_t e = r - rows1;
+                if (!pt[e]) return;
                 t = e / S2;
-                b = e - t * S2;
+                b0 = e - t * S2;
                 fixed_a = false;
             }
             const float* xt_ft = XT + ((uint64_t)f * M + t) * S2 * S2;
-            if (!exact_pass) {
-                // row bound: every component at least the item's, same float order
-                const float nx = mx[(uint64_t)f * M + t];
-                float ub;
-                if (fixed_a) {
-                    const float2 ea = Etab[(uint64_t)f * S2 + a];
-                    ub = Gk[(uint64_t)f * S2 + a] + gmax[t] + nx +
-                         K * ((ea.y + mx[M * M + t]) * nv + ea.x + mx[M * M + M + t]);
-                } else {
-                    const float2 eb = Etab[(uint64_t)t * S2 + b];
-                    ub = gmax[f] + Gk[(uint64_t)t * S2 + b] + nx +
-                         K * ((mx[M * M + f] + eb.y) * nv + mx[M * M + M + f] + eb.x);
+            const bool cross = (chmask[f] & chmask[t]) != 0ull;   // disjoint channels: X_ft == 0
+            const float* gt = (gstaged ? gst : Gk) + (uint64_t)t * S2;
+            const float2* et = Etab + (uint64_t)t * S2;
+            for (uint32_t x0 = 0; x0 < S2; x0 += 32 * kRowUnroll) {
+                bool ok[kRowUnroll];
+                float g2[kRowUnroll], xv[kRowUnroll];
+                float2 e2[kRowUnroll];
+#pragma unroll
+                for (int q = 0; q < kRowUnroll; ++q) {
+                    const uint32_t x = x0 + lane + 32 * q;
+                    const uint32_t a = fixed_a ? a0 : x, b = fixed_a ? x : b0;
+                    bool v = x < S2;
+                    if (v) v = fixed_a ? (fa[b] & 1) != 0 : fa[a] == 1;
+                    v = v && (a > b ? a - b : b - a) <= W;
+                    ok[q] = v;
+                    g2[q] = v ? gt[b] : 0.f;
+                    e2[q] = make_float2(v ? reinterpret_cast<const float*>(et)[2 * b] : 0.f, 0.f);
+                    xv[q] = (v && cross) ? xt_ft[(uint64_t)a * S2 + b] : 0.f;
                 }
-                if (ub < thr) { ubm = -INFINITY; return; }
-            }
-            for (uint32_t x = lane; x < S2; x += 32) {
-                if (fixed_a) {
-                    b = x;
-                    if (!(fa[b] & 1)) continue;
-                } else {
-                    a = x;
-                    if (fa[a] != 1) continue;
-                }
-                if ((a > b ? a - b : b - a) > W) continue;
-                const float2 ea = Etab[(uint64_t)f * S2 + a], eb = Etab[(uint64_t)t * S2 + b];
-                const float est = Gk[(uint64_t)f * S2 + a] + Gk[(uint64_t)t * S2 + b] - xt_ft[(uint64_t)a * S2 + b];
-                const float bound = K * ((ea.y + eb.y) * nv + ea.x + eb.x);
-                if (!exact_pass) {
-                    lbm = fmaxf(lbm, est - bound);
-                    ubm = fmaxf(ubm, est + bound);
-                    ++item_n;
-                    continue;
-                }
-                if (est + bound < thr) continue;
-                const uint32_t slot = atomicAdd(&s_ncand, 1u);
-                if (slot < (uint32_t)kCandCap) {
-                    cand[3 * slot] = a;
-                    cand[3 * slot + 1] = t;
-                    cand[3 * slot + 2] = b;
-                } else {
-                    score(a, t, b, kb);   // list full: score in place
+#pragma unroll
+                for (int q = 0; q < kRowUnroll; ++q) {
+                    if (!ok[q]) continue;
+                    const uint32_t x = x0 + lane + 32 * q;
+                    const uint32_t a = fixed_a ? a0 : x, b = fixed_a ? x : b0;
+                    const float2 ea = eft[a];
+                    const float est = gf[a] + g2[q] - xv[q];
+                    const float sb = __fsqrt_ru(e2[q].x);   // rounded up: the bound stays an upper bound
+                    const float bound = K * ((ea.y + sb) * nv + ea.x + e2[q].x);
+                    if (!listing) {
+                        lbm = fmaxf(lbm, est - bound);
+                        ubm = fmaxf(ubm, est + bound);
+                        ++item_n;
+                        continue;
+                    }
+                    if (est + bound < thr) continue;
+                    const uint32_t slot = atomicAdd(&sh.ncand, 1u);
+                    if (slot < (uint32_t)kCandCap) {
+                        cand[3 * slot] = a;
+                        cand[3 * slot + 1] = t;
+                        cand[3 * slot + 2] = b;
+                    } else {
+                        const uint32_t g = atomicAdd(&status->cand_count, 1u);
+                        if (g < gcand_cap)
+                            gcand[g] = ((unsigned long long)kk << 32) | ((unsigned long long)t << 20) |
+                                       ((unsigned long long)a << 10) | (unsigned long long)b;
+                        else
+                            sh.gfull = 1;
+                    }
                 }
             }
         };
+        // ---- phase B2: a quick lower bound from the highest-bound row of each
+        // warp's share, then keep only rows whose bound reaches it
         float lb = -INFINITY;
-        unsigned long long kbest = 0ull;
-        const float thr0 = fmaxf(seed, 0.f);
-        for (uint32_t row = warp; row < rows; row += nwarps) {
+        if (!overflow && nrows > 0) {
+            float bu = -INFINITY;
+            uint32_t bi = 0xFFFFFFFFu;
+            for (uint32_t i = warp + nwarps * lane; i < nrows; i += nwarps * 32)
+                if (rowmax[i] > bu) { bu = rowmax[i]; bi = i; }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ou = __shfl_xor_sync(0xffffffffu, bu, off);
+                const uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (ou > bu || (ou == bu && oi < bi)) { bu = ou; bi = oi; }
+            }
+            if (bi != 0xFFFFFFFFu) {
+                float lbm = -INFINITY, ubm = -INFINITY;
+                row_items(rows[bi], thr0, false, lbm, ubm);
+                lb = lbm;
+            }
+        }
+        {
+            const float lb1 = RF(tmp.rf).Reduce(lb, cub::Max());
+            if (threadIdx.x == 0) sh.lb = lb1;
+            __syncthreads();
+            const float thr1 = fmaxf(sh.lb, thr0);
+            if (!overflow) {
+                // compact the rows reaching thr1 (order kept), reusing the row arrays in place
+                uint32_t base = 0;
+                for (uint32_t i0 = 0; i0 < nrows; i0 += blockDim.x) {
+                    const uint32_t i = i0 + threadIdx.x;
+                    const bool keep = i < nrows && rowmax[i] >= thr1;
+                    const uint32_t r = keep ? rows[i] : 0u;
+                    uint32_t off, tot;
+                    SC(tmp.sc).ExclusiveSum(keep ? 1u : 0u, off, tot);
+                    __syncthreads();
+                    if (keep) rows[base + off] = r;
+                    base += tot;
+                    __syncthreads();
+                }
+                nrows = base;
+            }
+        }
+        // ---- phase C: lower bound and per-row upper bounds
+        for (uint32_t i = warp; i < nrows; i += nwarps) {
+            const uint32_t r = overflow ? i : rows[i];
             float lbm = -INFINITY, ubm = -INFINITY;
-            row_scan(row, thr0, false, lbm, ubm, kbest);
+            row_items(r, thr0, false, lbm, ubm);
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) ubm = fmaxf(ubm, __shfl_xor_sync(0xffffffffu, ubm, off));
-            if (keep_rows && lane == 0) rowmax[row] = ubm;
+            if (!overflow && lane == 0) rowmax[i] = ubm;
             lb = fmaxf(lb, lbm);
         }
         const float lbs = RF(tmp.rf).Reduce(lb, cub::Max());
-        if (threadIdx.x == 0) { sh.lb = lbs; s_ncand = 0; }
+        if (threadIdx.x == 0) sh.lb = lbs;
         __syncthreads();
         const float thr = fmaxf(fmaxf(sh.lb, seed), 0.f);
-        for (uint32_t row = warp; row < rows; row += nwarps) {
-            if (keep_rows && rowmax[row] < thr) continue;
+        // ---- phase D: candidate list
+        for (uint32_t i = warp; i < nrows; i += nwarps) {
+            if (!overflow && rowmax[i] < thr) continue;
             float lbm, ubm;
-            row_scan(row, thr, true, lbm, ubm, kbest);
+            row_items(overflow ? i : rows[i], thr, true, lbm, ubm);
         }
         __syncthreads();
-        const uint32_t nc = min(s_ncand, (uint32_t)kCandCap);
-        for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) score(cand[3 * i], cand[3 * i + 1], cand[3 * i + 2], kbest);
+        const uint32_t ncand = sh.ncand;
+        unsigned long long kbest = 0ull;
+        // hand the listed candidates to the scoring kernel (the listing already
+        // spilled past kCandCap straight into the global list)
+        const uint32_t nlisted = min(ncand, (uint32_t)kCandCap);
+        if (threadIdx.x == 0) s_gbase = atomicAdd(&status->cand_count, nlisted);
+        __syncthreads();
+        const uint32_t gbase = s_gbase;
+        const bool handed = (uint64_t)gbase + nlisted <= gcand_cap && !sh.gfull;
+        if (handed) {
+            for (uint32_t i = threadIdx.x; i < nlisted; i += blockDim.x)
+                gcand[gbase + i] = ((unsigned long long)kk << 32) | ((unsigned long long)cand[3 * i + 1] << 20) |
+                                   ((unsigned long long)cand[3 * i] << 10) | (unsigned long long)cand[3 * i + 2];
+        } else {
+            // the global list is full: mark this window's slots in it empty and
+            // score every item of the reaching rows here
+            for (uint64_t i = (uint64_t)gbase + threadIdx.x; i < gcand_cap && i < (uint64_t)gbase + nlisted;
+                 i += blockDim.x)
+                gcand[i] = ~0ull;
+            for (uint32_t i = threadIdx.x; i < nrows; i += blockDim.x) {
+                const uint32_t r = overflow ? i : rows[i];
+                uint32_t a = 0, t, b = 0;
+                bool fixed_a;
+                if (r < rows1) { a = alist[r / M]; t = r % M; fixed_a = true; }
+                else { const uint32_t e = r - rows1; if (!pt[e]) continue; t = e / S2; b = e - t * S2; fixed_a = false; }
+                for (uint32_t x = 0; x < S2; ++x) {
+                    if (fixed_a) { b = x; if (!(fa[b] & 1)) continue; } else { a = x; if (fa[a] != 1) continue; }
+                    if ((a > b ? a - b : b - a) > W) continue;
+                    const float2 ea = eft[a], eb = Etab[(uint64_t)t * S2 + b];
+                    const float est = gf[a] + Gk[(uint64_t)t * S2 + b] -
+                                      XT[(((uint64_t)f * M + t) * S2 + a) * S2 + b];
+                    const float bound = K * ((ea.y + eb.y) * nv + ea.x + eb.x);
+                    if (est + bound < thr) continue;
+                    const float v = pair_exact_g(d, T, V, f, t, p, a, b);
+                    ++exact_n;
+                    if (!(v > 0.f)) continue;
+                    const uint64_t rr0 = (uint64_t)t + (uint64_t)M * a + (uint64_t)M * S2 * b;
+                    uint32_t pr = item_priority(rr0, d.WG, lbits);
+                    for (uint64_t rr = rr0 + items; rr < slots; rr += items) {
+                        const uint32_t p2 = item_priority(rr, d.WG, lbits);
+                        pr = p2 < pr ? p2 : pr;
+                    }
+                    const unsigned long long key =
+                        ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - pr);
+                    kbest = key > kbest ? key : kbest;
+                }
+            }
+        }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             const unsigned long long o = __shfl_down_sync(0xffffffffu, kbest, off);
@@ -494,6 +639,47 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
     if (item_n) atomicAdd(&status->pair_items, item_n);
 }
 
+// Exact scores of the listed candidates, one thread each: entry = window slot
+// kk (32 bits) | t (12) | a (10) | b (10).  Folds the canonical winner key into
+// keys[k0 + kk].
+__global__ void __launch_bounds__(256) score_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
+                                                    const uint32_t* __restrict__ flag, uint32_t k0,
+                                                    const uint32_t* __restrict__ best_lab,
+                                                    const uint32_t* __restrict__ best_idx,
+                                                    const unsigned long long* __restrict__ gcand, uint32_t cap,
+                                                    DevStatus* status, unsigned long long* keys)
+{
+    const uint32_t n = min(status->cand_count, cap);
+    const uint32_t S2 = 2 * d.S + 1, M = d.M;
+    const uint64_t items = (uint64_t)S2 * S2 * M;
+    const uint64_t nloc = (items - 1) / d.WG + 1;
+    const uint64_t slots = nloc * d.WG;
+    uint32_t lbits = 0;
+    while ((1u << lbits) < d.WG) ++lbits;
+    uint32_t done = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long e = gcand[i];
+        if (e == ~0ull) continue;
+        const uint32_t kk = (uint32_t)(e >> 32);
+        const uint32_t t = (uint32_t)(e >> 20) & 0xFFFu, a = (uint32_t)(e >> 10) & 0x3FFu, b = (uint32_t)e & 0x3FFu;
+        if ((uint64_t)k0 + kk >= status->n_flag || t >= M || a >= S2 || b >= S2) continue;
+        const uint32_t id = flag[k0 + kk];
+        const uint32_t f = best_lab[id], p = best_idx[id];
+        const float acc = pair_exact_g(d, T, V, f, t, p, a, b);
+        ++done;
+        if (!(acc > 0.f)) continue;
+        const uint64_t r = (uint64_t)t + (uint64_t)M * a + (uint64_t)M * S2 * b;
+        uint32_t pr = item_priority(r, d.WG, lbits);
+        for (uint64_t rr = r + items; rr < slots; rr += items) {
+            const uint32_t p2 = item_priority(rr, d.WG, lbits);
+            pr = p2 < pr ? p2 : pr;
+        }
+        atomicMax(&keys[k0 + kk],
+                  ((unsigned long long)__float_as_uint(acc) << 32) | (unsigned long long)(0xFFFFFFFFu - pr));
+    }
+    if (done) atomicAdd(&status->n_pair_exact, done);
+}
+
 }  // namespace
 
 int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStream_t st)
@@ -501,13 +687,15 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     const Layout& L = *w.lay;
     if (!L.screened) return FBP_OK;
     const uint32_t S2 = 2 * d.S + 1;
+    count_launch(4);
     energy_table_kernel<<<(d.M * S2 + 255) / 256, 256, 0, st>>>(d, T, w.at<float2>(L.off_et));
     const size_t smem = (size_t)2 * d.C * d.W * 4 + 8 + (size_t)kLagChunk * (d.W + 1) * 8;
     if (smem > 200 * 1024) return fail(FBP_E_ARG, "template too large for the pair table kernel");
     FBP_CUDA(cudaFuncSetAttribute(cross_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cross_table_kernel<<<d.M * d.M, 256, smem, st>>>(d, T, w.at<float>(L.off_xt), w.at<float>(L.off_mx));
     energy_max_kernel<<<(d.M + 127) / 128, 128, 0, st>>>(d, w.at<float2>(L.off_et), w.at<float>(L.off_mx) + (size_t)d.M * d.M);
-    template_order_kernel<<<1, 256, d.M * 4, st>>>(d, T, w.at<uint32_t>(L.off_perm));
+    template_order_kernel<<<1, 256, d.M * 4, st>>>(d, T, w.at<uint32_t>(L.off_perm),
+                                                  reinterpret_cast<unsigned long long*>(w.at<uint32_t>(L.off_perm) + ((d.M + 1) & ~1u)));
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }
@@ -519,7 +707,7 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     if (!L.screened) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     if (nflag_max == 0) return FBP_OK;
     const uint32_t S2 = 2 * d.S + 1;
-    if (S2 > 1024 || d.C > 256) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
+    if (S2 > 1024 || d.C > 256 || d.M > 4096) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     FBP_CUDA(cudaMemsetAsync(w.keys(), 0, sizeof(unsigned long long) * nflag_max, st));
     const uint32_t SL = (2 * d.S + d.W + 3) & ~3u, Wp = (d.W + 3) & ~3u;
     const size_t strip = (size_t)d.C * SL * 4, per_t = (size_t)d.C * Wp * 4;
@@ -527,9 +715,10 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     while (Q > 1 && strip + Q * per_t > 200 * 1024) Q >>= 1;
     const size_t smem_a = strip + Q * per_t;
     if (smem_a > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
-    const size_t smem_b = ((S2 + 15) & ~15u) + (((size_t)d.M * S2 + 15) & ~(size_t)15) + (size_t)S2 * 4 +
-                          (size_t)d.M * S2 * 4 + (size_t)kRowCap * 4 + (size_t)d.C * d.W * 4 + (size_t)d.M * 4 +
-                          (size_t)kCandCap * 12;
+    const size_t gstage = (size_t)d.M * S2 * 4 <= 48 * 1024 ? (size_t)d.M * S2 * 4 : 0;
+    const size_t smem_b = (((size_t)S2 + 3) & ~(size_t)3) * 4 + (size_t)S2 * 8 + (size_t)4 * d.M * 4 +
+                          (size_t)d.C * d.W * 4 + (size_t)kRowCap * 8 + (size_t)kCandCap * 12 + (size_t)S2 * 4 +
+                          (((size_t)S2 + 15) & ~(size_t)15) + (((size_t)d.M * S2 + 15) & ~(size_t)15) + gstage + 80;
     if (smem_b > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     FBP_CUDA(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
     const uint32_t threads_a = (S2 + 31) & ~31u;
@@ -538,15 +727,19 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     const float2* Et = w.at<float2>(L.off_et);
     const float* XT = w.at<float>(L.off_xt);
     const uint32_t* perm = w.at<uint32_t>(L.off_perm);
+    const unsigned long long* chm = reinterpret_cast<const unsigned long long*>(perm + ((d.M + 1) & ~1u));
     for (uint32_t k0 = 0; k0 < nflag_max; k0 += (uint32_t)L.gbatch) {
         const uint32_t kc = (uint32_t)((nflag_max - k0) < L.gbatch ? (nflag_max - k0) : L.gbatch);
         dim3 ga(kc, groups);
 #define FBP_PC(QQ)                                                                                       \
     case QQ:                                                                                             \
         FBP_CUDA(cudaFuncSetAttribute(partial_corr_kernel<QQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a)); \
-        partial_corr_kernel<QQ><<<ga, threads_a, smem_a, st>>>(d, V, T, w.L(), theta, Et, perm, w.flag(), w.status(), \
+        partial_corr_kernel<QQ><<<ga, threads_a, smem_a, st>>>(d, V, T, w.L(), theta, Et, perm, chm, w.flag(), w.status(), \
                                                               w.best_lab(), w.best_idx(), k0, G);        \
         break;
+        count_launch(3);
+        {
+        KScope ks(&fbp_chunk_stats::ms_partial_corr, st);
         switch (Q) {
             FBP_PC(8)
             FBP_PC(4)
@@ -554,10 +747,19 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
             FBP_PC(1)
         }
 #undef FBP_PC
+        }
         const uint32_t gb = kc < 148u * 8 ? kc : 148u * 8;
+        FBP_CUDA(cudaMemsetAsync(&w.status()->cand_count, 0, 4, st));
+        unsigned long long* gcand = w.at<unsigned long long>(L.off_cand);
+        {
+        KScope ks(&fbp_chunk_stats::ms_screen, st);
         screen_kernel<<<gb, kScrThreads, smem_b, st>>>(d, V, T, w.L(), theta, Et, XT, G, k0, kc, w.flag(), w.status(),
                                                        w.best_lab(), w.best_idx(), w.best_lik(), w.keys(),
-                                                       w.at<float>(L.off_mx));
+                                                       w.at<float>(L.off_mx), gcand, (uint32_t)L.cand_cap, chm);
+        }
+        KScope ks(&fbp_chunk_stats::ms_score, st);
+        score_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, w.flag(), k0, w.best_lab(), w.best_idx(), gcand,
+                                              (uint32_t)L.cand_cap, w.status(), w.keys());
         FBP_CUDA(cudaGetLastError());
     }
     return FBP_OK;

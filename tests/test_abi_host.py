@@ -35,7 +35,7 @@ def test_header_declares_exports():
 def test_library_exports_every_declared_symbol(lib):
     for name in declared_functions():
         assert hasattr(lib, name), name
-    assert lib.fbp_abi_version() == 1
+    assert lib.fbp_abi_version() == 2
 
 
 def test_workspace_bytes(lib):

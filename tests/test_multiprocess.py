@@ -1,0 +1,70 @@
+"""Sharding of independent segments across ranks (gloo, world size 2, CPU)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from spikesorting_fullpursuit_b200.segments import pursue_segments, shard_segments
+
+
+def test_shards_are_balanced_and_deterministic():
+    lengths = [50, 10, 40, 30, 30, 5, 60]
+    sh = shard_segments(lengths, 3)
+    assert sorted(i for s in sh for i in s) == list(range(len(lengths)))
+    loads = [sum(lengths[i] for i in s) for s in sh]
+    assert max(loads) - min(loads) <= max(lengths)
+    assert sh == shard_segments(lengths, 3)
+    assert shard_segments(lengths, 1) == [list(range(len(lengths)))]
+    with pytest.raises(ValueError):
+        shard_segments(lengths, 0)
+
+
+def _fake_pursue(voltage, tag):
+    # deterministic stand-in for binary_pursuit: indices of threshold crossings
+    idx = np.flatnonzero(voltage[0] > 2.0).astype(np.int64)
+    return idx, np.full(idx.size, tag, dtype=np.int64)
+
+
+def _segments():
+    rng = np.random.default_rng(3)
+    return [(rng.standard_normal((2, n)).astype(np.float32), k) for k, n in enumerate([900, 300, 700, 500, 100])]
+
+
+def _worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        res = pursue_segments(_segments(), pursue=_fake_pursue)
+        out[rank] = [(r[0].tolist(), r[1].tolist()) for r in res]
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_two_ranks_gather_every_segment_in_order():
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        want = [(_fake_pursue(*seg)[0].tolist(), _fake_pursue(*seg)[1].tolist()) for seg in _segments()]
+        assert out[0] == want
+        assert out[1] == want
+
+
+def test_without_process_group_runs_locally():
+    res = pursue_segments(_segments(), pursue=_fake_pursue)
+    assert len(res) == 5 and all(r[1][0] == k for k, r in enumerate(res) if r[1].size)
