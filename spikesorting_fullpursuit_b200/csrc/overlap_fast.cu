@@ -17,6 +17,8 @@
 // therefore the reference's.
 #include <cub/cub.cuh>
 
+#include <vector>
+
 #include "fbp_internal.cuh"
 
 namespace fbp {
@@ -154,91 +156,161 @@ __device__ __forceinline__ bool window_skipped(const Dims& d, const float* L, co
 }
 
 // Partial correlations G[k][t][b] = X_t(b) - 0.5 Et[t][b] of every template
-// with the flagged window (masked to [p, p+W)).  One CTA per (window, group
-// of Q templates in perm order), one thread per shift b.
+// with each flagged window (masked to [p, p+W)).  A CTA owns one group of Q
+// templates (in perm order; only the group's union of non-zero channels is
+// staged) and walks over the windows kPcWin at a time.  Lane = (window, shift
+// sub-block): a warp covers 16 consecutive shifts of 8 windows, so the taps
+// that can meet the window's W live samples form one range per warp (the
+// zero triangle of the masked correlation is skipped), and each lane computes
+// 4 consecutive shifts for the Q templates from aligned 16-byte strip loads.
+// The strips keep their zero margins from one clearing; each window writes
+// only its W live samples per channel (cp.async).  The sums are estimates:
+// any order, FMA allowed.
+constexpr int kPcR = 4;       // shifts per lane
+constexpr int kPcWin = 8;     // windows per CTA iteration (lane bits 2..4)
+constexpr int kPcPad = 20;    // zero margin around the live samples in a staged strip
+constexpr int kPcMaxWarps = 12;   // two CTAs of 12 warps fit an SM at <= 80 registers
+
+struct PcGeom {
+    uint32_t Wp, Z, SLc, WS;  // padded taps; strip index of window sample 0; strip length; window stride
+    int o;                    // shift b reads strip index b - o + j  (o = S - Z, a multiple of 4)
+};
+
+__host__ __device__ inline PcGeom pc_geom(const Dims& d, uint32_t Cu)
+{
+    PcGeom g;
+    g.Wp = (d.W + 3) & ~3u;
+    g.Z = kPcPad + (d.S & 3u);
+    g.o = (int)d.S - (int)g.Z;
+    g.SLc = (g.Z + d.W + kPcPad + 3) & ~3u;
+    uint32_t ws = Cu * g.SLc;
+    ws += (16u - ws % 32u + 32u) % 32u;   // windows 16 banks apart: a quarter-warp's two windows do not collide
+    g.WS = ws;
+    return g;
+}
+
+__host__ __device__ inline size_t pc_smem_bytes(const Dims& d, uint32_t Cu, int Q)
+{
+    const PcGeom g = pc_geom(d, Cu);
+    return ((size_t)Q * Cu * g.Wp + (size_t)kPcWin * g.WS) * 4;
+}
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src)
+{
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
+}
+
 template <int Q>
-__global__ void __launch_bounds__(1024) partial_corr_kernel(Dims d, const float* __restrict__ V,
-                                                            const float* __restrict__ T,
-                                                            const float* __restrict__ L,
-                                                            const float* __restrict__ theta,
-                                                            const float2* __restrict__ Et,
-                                                            const uint32_t* __restrict__ perm,
-                                                            const unsigned long long* __restrict__ chmask,
-                                                            const uint32_t* __restrict__ flag,
-                                                            const DevStatus* status,
-                                                            const uint32_t* __restrict__ best_lab,
-                                                            const uint32_t* __restrict__ best_idx,
-                                                            uint32_t k0, float* G)
+__global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
+    Dims d, const float* __restrict__ V, const float* __restrict__ T, const float* __restrict__ L,
+    const float* __restrict__ theta, const float2* __restrict__ Et, const uint32_t* __restrict__ perm,
+    const unsigned long long* __restrict__ chmask, const uint32_t* __restrict__ flag, const DevStatus* status,
+    const uint32_t* __restrict__ best_lab, const uint32_t* __restrict__ best_idx, uint32_t k0, uint32_t kc,
+    float* G)
 {
     extern __shared__ __align__(16) float sm[];
     __shared__ uint32_t chans[256];
-    __shared__ uint32_t nch;
-    const uint32_t k = k0 + blockIdx.x;
-    if (k >= status->n_flag) return;
-    const uint32_t id = flag[k];
-    const uint32_t f = best_lab[id], p = best_idx[id];
-    if (window_skipped(d, L, theta, f, p)) return;
-    const uint32_t S2 = 2 * d.S + 1, W = d.W, C = d.C;
-    const uint32_t SL = (2 * d.S + W + 3) & ~3u;
-    const uint32_t Wp = (W + 3) & ~3u;
-    float* Vs = sm;                  // [C][SL] window masked into a zero strip
-    float* Ts = sm + C * SL;         // [Q][C][Wp]
-    const uint32_t tq = C * Wp;
+    __shared__ uint32_t s_nch;
+    __shared__ uint32_t s_p[kPcWin];
+    __shared__ int s_ok[kPcWin];
+    const uint32_t S2 = 2 * d.S + 1, W = d.W, M = d.M;
     const uint32_t g0 = blockIdx.y * Q;
-    for (uint32_t e = threadIdx.x; e < C * SL; e += blockDim.x) {
-        const uint32_t c = e / SL, y = e - c * SL;
-        Vs[e] = (y >= d.S && y < d.S + W) ? V[(uint64_t)c * d.N + p - d.S + y] : 0.f;
-    }
-    for (uint32_t e = threadIdx.x; e < Q * tq; e += blockDim.x) {
-        const uint32_t q = e / tq, r = e - q * tq, c = r / Wp, j = r - c * Wp;
-        const uint32_t gi = g0 + q;
-        Ts[e] = (gi < d.M && j < W) ? T[((uint64_t)perm[gi] * C + c) * W + j] : 0.f;
-    }
     if (threadIdx.x == 0) {
-        // channels where any template of the group is non-zero (order irrelevant for an estimate)
         unsigned long long m = 0ull;
         for (uint32_t q = 0; q < Q; ++q)
-            if (g0 + q < d.M) m |= chmask[perm[g0 + q]];
+            if (g0 + q < M) m |= chmask[perm[g0 + q]];
         uint32_t n = 0;
-        for (uint32_t c = 0; c < C; ++c)
+        for (uint32_t c = 0; c < d.C; ++c)
             if (c >= 64 || ((m >> c) & 1ull)) chans[n++] = c;
-        nch = n;
+        s_nch = n;
     }
     __syncthreads();
-    const uint32_t b = threadIdx.x;
-    if (b >= S2) return;
-    float acc[Q];
+    const uint32_t Cu = s_nch;
+    const PcGeom gm = pc_geom(d, Cu);
+    const uint32_t Wp = gm.Wp;
+    float* Ts = sm;                                   // [Q][Cu][Wp]
+    float* Vs = sm + (size_t)Q * Cu * Wp;              // [kPcWin][WS], row ci at ci * SLc
+    for (uint32_t e = threadIdx.x; e < Q * Cu * Wp; e += blockDim.x) {
+        const uint32_t q = e / (Cu * Wp), r = e - q * Cu * Wp, ci = r / Wp, j = r - ci * Wp;
+        Ts[e] = (g0 + q < M && j < W) ? T[((uint64_t)perm[g0 + q] * d.C + chans[ci]) * W + j] : 0.f;
+    }
+    for (uint32_t e = threadIdx.x; e < kPcWin * gm.WS; e += blockDim.x) Vs[e] = 0.f;
+    const uint32_t nflag = status->n_flag;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t wi = lane >> 2, bs = lane & 3;
+    for (uint32_t base = blockIdx.x * kPcWin; base < kc; base += gridDim.x * kPcWin) {
+        __syncthreads();
+        if (threadIdx.x < kPcWin) {
+            const uint32_t kk = base + threadIdx.x;
+            int ok = 0;
+            uint32_t p = 0;
+            if (kk < kc && k0 + kk < nflag) {
+                const uint32_t id = flag[k0 + kk];
+                const uint32_t f = best_lab[id];
+                p = best_idx[id];
+                ok = !window_skipped(d, L, theta, f, p);
+            }
+            s_ok[threadIdx.x] = ok;
+            s_p[threadIdx.x] = p;
+        }
+        __syncthreads();
+        for (uint32_t r = warp; r < kPcWin * Cu; r += nwarps) {
+            const uint32_t w = r / Cu, ci = r - w * Cu;
+            if (!s_ok[w]) continue;
+            const float* src = V + (uint64_t)chans[ci] * d.N + s_p[w];
+            float* dst = Vs + (size_t)w * gm.WS + (size_t)ci * gm.SLc + gm.Z;
+            for (uint32_t j = lane; j < W; j += 32) cp_async4(dst + j, src + j);
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+        if (!s_ok[wi]) continue;
+        float* Gk = G + (uint64_t)(base + wi) * M * S2;
+        const float* vw = Vs + (size_t)wi * gm.WS;
+        for (uint32_t bw = warp * 16; bw < S2; bw += nwarps * 16) {
+            const uint32_t b0 = bw + kPcR * bs;
+            int jlo = (int)d.S - (int)bw - 15;
+            jlo = jlo < 0 ? 0 : (jlo & ~3);
+            int jhi = ((int)(d.S + W) - (int)bw + 3) & ~3;
+            jhi = jhi > (int)Wp ? (int)Wp : jhi;
+            float acc[Q][kPcR];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) acc[q] = 0.f;
-    for (uint32_t ci = 0; ci < nch; ++ci) {
-        const uint32_t c = chans[ci];
-        const float* vr = Vs + c * SL + b;
-        const float* tr = Ts + c * Wp;
-        uint32_t j = 0;
-        for (; j + 4 <= W; j += 4) {
-            const float v0 = vr[j], v1 = vr[j + 1], v2 = vr[j + 2], v3 = vr[j + 3];
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 0; r < kPcR; ++r) acc[q][r] = 0.f;
+            const int vb = (int)b0 - gm.o;
+            for (uint32_t ci = 0; ci < Cu; ++ci) {
+                const float* vr = vw + (size_t)ci * gm.SLc;
+                const float* tr = Ts + (size_t)ci * Wp;
+                for (int j0 = jlo; j0 < jhi; j0 += 4) {
+                    const float4 va = *reinterpret_cast<const float4*>(vr + vb + j0);
+                    const float4 vc = *reinterpret_cast<const float4*>(vr + vb + j0 + 4);
+                    const float v[8] = {va.x, va.y, va.z, va.w, vc.x, vc.y, vc.z, vc.w};
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) {
+                        const float4 t4 = *reinterpret_cast<const float4*>(tr + (size_t)q * Cu * Wp + j0);
+#pragma unroll
+                        for (int r = 0; r < kPcR; ++r) {
+                            float a = acc[q][r];
+                            a = fmaf(t4.x, v[r], a);
+                            a = fmaf(t4.y, v[r + 1], a);
+                            a = fmaf(t4.z, v[r + 2], a);
+                            a = fmaf(t4.w, v[r + 3], a);
+                            acc[q][r] = a;
+                        }
+                    }
+                }
+            }
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
-                const float4 t4 = *reinterpret_cast<const float4*>(tr + q * tq + j);
-                acc[q] = fmaf(t4.x, v0, acc[q]);
-                acc[q] = fmaf(t4.y, v1, acc[q]);
-                acc[q] = fmaf(t4.z, v2, acc[q]);
-                acc[q] = fmaf(t4.w, v3, acc[q]);
+                if (g0 + q >= M) continue;
+                const uint32_t t = perm[g0 + q];
+#pragma unroll
+                for (int r = 0; r < kPcR; ++r) {
+                    const uint32_t bb = b0 + r;
+                    if (bb < S2) Gk[(uint64_t)t * S2 + bb] = acc[q][r] - 0.5f * Et[(uint64_t)t * S2 + bb].x;
+                }
             }
-        }
-        for (; j < W; ++j) {
-            const float v = vr[j];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) acc[q] = fmaf(tr[q * tq + j], v, acc[q]);
-        }
-    }
-    float* Gk = G + (uint64_t)(k - k0) * d.M * S2;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const uint32_t gi = g0 + q;
-        if (gi < d.M) {
-            const uint32_t t = perm[gi];
-            Gk[(uint64_t)t * S2 + b] = acc[q] - 0.5f * Et[(uint64_t)t * S2 + b].x;
         }
     }
 }
@@ -682,6 +754,17 @@ __global__ void __launch_bounds__(256) score_kernel(Dims d, const float* __restr
 
 }  // namespace
 
+struct PcConfig {
+    int Q = 0;
+    size_t smem = 0;
+};
+
+PcConfig& pc_config()
+{
+    static thread_local PcConfig c;
+    return c;
+}
+
 int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStream_t st)
 {
     const Layout& L = *w.lay;
@@ -697,6 +780,32 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     template_order_kernel<<<1, 256, d.M * 4, st>>>(d, T, w.at<uint32_t>(L.off_perm),
                                                   reinterpret_cast<unsigned long long*>(w.at<uint32_t>(L.off_perm) + ((d.M + 1) & ~1u)));
     FBP_CUDA(cudaGetLastError());
+    // channel unions of the template groups decide how many templates a
+    // partial-correlation CTA can stage: read the order and masks back once
+    std::vector<uint32_t> perm(d.M);
+    std::vector<unsigned long long> mask(d.M);
+    FBP_CUDA(cudaMemcpyAsync(perm.data(), w.at<uint32_t>(L.off_perm), d.M * 4, cudaMemcpyDeviceToHost, st));
+    FBP_CUDA(cudaMemcpyAsync(mask.data(), w.at<uint32_t>(L.off_perm) + ((d.M + 1) & ~1u), d.M * 8,
+                             cudaMemcpyDeviceToHost, st));
+    FBP_CUDA(cudaStreamSynchronize(st));
+    PcConfig& pc = pc_config();
+    pc.Q = 0;
+    for (int Q = 8; Q >= 1; Q >>= 1) {
+        uint32_t cu_max = 0;
+        for (uint32_t g0 = 0; g0 < d.M; g0 += Q) {
+            unsigned long long m = 0ull;
+            for (uint32_t q = 0; q < (uint32_t)Q && g0 + q < d.M; ++q) m |= mask[perm[g0 + q]];
+            uint32_t cu = 0;
+            for (uint32_t c = 0; c < d.C; ++c) cu += (c >= 64 || ((m >> c) & 1ull)) ? 1u : 0u;
+            cu_max = cu > cu_max ? cu : cu_max;
+        }
+        const size_t smem = pc_smem_bytes(d, cu_max, Q);
+        if (smem <= 110 * 1024 || (Q == 1 && smem <= 200 * 1024)) {
+            pc.Q = Q;
+            pc.smem = smem;
+            break;
+        }
+    }
     return FBP_OK;
 }
 
@@ -709,19 +818,17 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     const uint32_t S2 = 2 * d.S + 1;
     if (S2 > 1024 || d.C > 256 || d.M > 4096) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     FBP_CUDA(cudaMemsetAsync(w.keys(), 0, sizeof(unsigned long long) * nflag_max, st));
-    const uint32_t SL = (2 * d.S + d.W + 3) & ~3u, Wp = (d.W + 3) & ~3u;
-    const size_t strip = (size_t)d.C * SL * 4, per_t = (size_t)d.C * Wp * 4;
-    int Q = 8;
-    while (Q > 1 && strip + Q * per_t > 200 * 1024) Q >>= 1;
-    const size_t smem_a = strip + Q * per_t;
-    if (smem_a > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
+    const PcConfig pc = pc_config();
+    const int Q = pc.Q;
+    const size_t smem_a = pc.smem;
+    if (Q == 0) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
+    const uint32_t pc_threads = 32u * std::min<uint32_t>((S2 + 15) / 16, kPcMaxWarps);
     const size_t gstage = (size_t)d.M * S2 * 4 <= 48 * 1024 ? (size_t)d.M * S2 * 4 : 0;
     const size_t smem_b = (((size_t)S2 + 3) & ~(size_t)3) * 4 + (size_t)S2 * 8 + (size_t)4 * d.M * 4 +
                           (size_t)d.C * d.W * 4 + (size_t)kRowCap * 8 + (size_t)kCandCap * 12 + (size_t)S2 * 4 +
                           (((size_t)S2 + 15) & ~(size_t)15) + (((size_t)d.M * S2 + 15) & ~(size_t)15) + gstage + 80;
     if (smem_b > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     FBP_CUDA(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
-    const uint32_t threads_a = (S2 + 31) & ~31u;
     const uint32_t groups = (d.M + Q - 1) / Q;
     float* G = w.at<float>(L.off_g);
     const float2* Et = w.at<float2>(L.off_et);
@@ -730,16 +837,23 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     const unsigned long long* chm = reinterpret_cast<const unsigned long long*>(perm + ((d.M + 1) & ~1u));
     for (uint32_t k0 = 0; k0 < nflag_max; k0 += (uint32_t)L.gbatch) {
         const uint32_t kc = (uint32_t)((nflag_max - k0) < L.gbatch ? (nflag_max - k0) : L.gbatch);
-        dim3 ga(kc, groups);
-#define FBP_PC(QQ)                                                                                       \
-    case QQ:                                                                                             \
-        FBP_CUDA(cudaFuncSetAttribute(partial_corr_kernel<QQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a)); \
-        partial_corr_kernel<QQ><<<ga, threads_a, smem_a, st>>>(d, V, T, w.L(), theta, Et, perm, chm, w.flag(), w.status(), \
-                                                              w.best_lab(), w.best_idx(), k0, G);        \
-        break;
         count_launch(3);
         {
         KScope ks(&fbp_chunk_stats::ms_partial_corr, st);
+        // persistent over the windows: as many CTAs as fit resident, split over the template groups
+#define FBP_PC(QQ)                                                                                            \
+    case QQ: {                                                                                                \
+        FBP_CUDA(cudaFuncSetAttribute(partial_corr_kernel<QQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                      (int)smem_a));                                                          \
+        int per_sm = 1;                                                                                       \
+        FBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, partial_corr_kernel<QQ>,              \
+                                                               (int)pc_threads, smem_a));                 \
+        const uint32_t want = (uint32_t)((148u * (per_sm > 0 ? per_sm : 1) + groups - 1) / groups);           \
+        const uint32_t slices = std::min<uint32_t>((kc + kPcWin - 1) / kPcWin, want);                         \
+        partial_corr_kernel<QQ><<<dim3(slices, groups), pc_threads, smem_a, st>>>(                          \
+            d, V, T, w.L(), theta, Et, perm, chm, w.flag(), w.status(), w.best_lab(), w.best_idx(), k0, kc, G); \
+        break;                                                                                                \
+    }
         switch (Q) {
             FBP_PC(8)
             FBP_PC(4)
