@@ -100,15 +100,16 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
     L->off_blk = take(L->nblk * 4);
     L->off_status = take(sizeof(DevStatus));
     if (!(flags & FBP_PLAIN_FP32)) {
-        // tensor-core likelihood: bf16 hi/lo copies of the voltage (sample-major,
-        // channels padded to a multiple of 8) and of the templates, plus the
-        // queue of samples to recompute exactly.
+        // tensor-core likelihood: the voltage sample-major in 4-channel rows
+        // (channels padded to a multiple of 8), the templates in MMA order and
+        // with taps padded to a multiple of 4, plus the queue of sample runs to
+        // recompute exactly.
         L->Cp = (C + 7) / 8 * 8;
-        L->Kt = W;
         L->Mp = (M + 15) / 16 * 16;
         L->vq_rows = N + 256 + 2 * W;
         L->off_vt_hi = take(L->vq_rows * L->Cp * 4);   // voltage as [Cp/4][rows][4] fp32
         L->off_tt_hi = take(L->Mp * W * L->Cp * 4);    // templates as [W][Cp/8][2][Mp][4] fp32
+        L->off_tpad = take(M * C * ((W + 3) / 4 * 4) * 4);   // templates as [M][C][W rounded up to 4]
         L->off_tnorm = take(M * C * 4);
         uint64_t cap = M * N / 4;
         if (cap > (32ull << 20)) cap = 32ull << 20;
@@ -272,7 +273,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         FBP_CUDA(cudaStreamSynchronize(st));
         if (hs.error) return fail(FBP_E_DEVICE, "device status error " + std::to_string(hs.error));
         if (overlap) S.flagged += hs.n_flag;
-        S.fixups += hs.n_fix;
+        S.fixups += 4ull * hs.n_fix;   // runs of 4 samples
         const uint32_t n = hs.n_spikes;
         if (n == 0) break;
         if ((uint64_t)total + n > capacity) return fail(FBP_E_CAPACITY, "spike capacity exceeded");

@@ -57,7 +57,7 @@ struct DevStatus {
     uint32_t n_next;        // windows listed for the next pass
     uint32_t chain_overflow;// a prune/reassign chain was longer than the walk limit
     uint32_t error;         // nonzero: a kernel detected an inconsistent state
-    uint32_t n_fix;         // likelihood samples queued for exact recomputation
+    uint32_t n_fix;         // runs of 4 likelihood samples queued for exact recomputation
     uint32_t n_pair_exact;  // overlap items recomputed exactly
     uint32_t n_conf;        // spikes of this pass overlapping an earlier one
     unsigned long long pair_items;  // items evaluated by the overlap recheck
@@ -75,8 +75,8 @@ struct Layout {
     size_t off_has, off_newval, off_pidx, off_plab, off_pwin, off_pconf, off_keys;
     size_t off_blk, off_status;
     // tensor-core likelihood (mode 1)
-    size_t off_vt_hi, off_vt_lo, off_tt_hi, off_tt_lo, off_fix, off_tnorm;
-    uint64_t Cp, Kt, Mp, n_fix_cap, vq_rows;
+    size_t off_vt_hi, off_tt_hi, off_tpad, off_fix, off_tnorm;
+    uint64_t Cp, Mp, n_fix_cap, vq_rows;
     // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
     // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
     // template processing order perm[M]

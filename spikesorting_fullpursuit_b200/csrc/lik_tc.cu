@@ -136,6 +136,7 @@ struct TcParams {
     const float* Tq;      // [W][Cq/2][2][Np][4]
     const float* bias;    // [M]
     const float* tnorm;   // [M][C] channel norms of the templates
+    const float* Tp;      // [M][C][Wp] templates, taps padded to a multiple of 4 (exact recomputation)
     const uint32_t* list; // listed windows (mode 1) or null (mode 0: contiguous tiles)
     uint32_t nitems;      // tiles (mode 0) or listed windows (mode 1)
     uint32_t rows;        // rows of each Vq channel block
@@ -292,27 +293,36 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
                 for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
                     float v[16];
                     tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
-                    if (!valid) continue;
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
                         const uint32_t t = cg * 16 + e;
-                        if (t >= d.M) continue;
-                        float out;
-                        if ((uint64_t)s + d.W >= d.N) {
-                            out = 0.f;
-                        } else {
-                            const float b = sbias[t];
-                            const float est = v[e] + b;
-                            out = est;
-                            if (!(est + bnd[i * d.M + t] <= 0.f)) {
-                                const uint32_t slot = atomicAdd(&P.status->n_fix, 1u);
-                                if (slot < P.fix_cap)
-                                    P.fix[slot] = ((unsigned long long)t << 32) | s;
-                                else
-                                    out = exact_likelihood(d, P.V, P.T, b, t, s);
-                            }
+                        if (t >= d.M) continue;   // uniform over the warp
+                        const bool live = valid && (uint64_t)s + d.W < d.N;
+                        const float b = sbias[t];
+                        const float est = v[e] + b;
+                        const bool need = live && !(est + bnd[i * d.M + t] <= 0.f);
+                        // queue the warp's samples needing an exact value as runs of 4
+                        // consecutive rows (one entry per non-empty nibble of the ballot)
+                        const uint32_t m = __ballot_sync(0xffffffffu, need);
+                        if (m == 0u) {
+                            if (valid) P.L[(uint64_t)t * d.N + s] = live ? est : 0.f;
+                            continue;
                         }
-                        P.L[(uint64_t)t * d.N + s] = out;
+                        uint32_t nz = 0;   // bit k: nibble k non-empty
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
+                        uint32_t base = 0;
+                        if (lane == 0) base = atomicAdd(&P.status->n_fix, (uint32_t)__popc(nz));
+                        base = __shfl_sync(0xffffffffu, base, 0);
+                        const uint32_t k = lane >> 2;
+                        const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
+                        const bool queued = ((nz >> k) & 1u) && slot < P.fix_cap;
+                        if ((lane & 3u) == 0 && queued)
+                            P.fix[slot] = ((unsigned long long)t << 40) |
+                                          ((unsigned long long)((m >> (4 * k)) & 0xFu) << 32) | s;
+                        float out = live ? est : 0.f;
+                        if (need && !queued) out = exact_likelihood(d, P.V, P.T, b, t, s);
+                        if (valid) P.L[(uint64_t)t * d.N + s] = out;
                     }
                 }
             }
@@ -330,16 +340,60 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
     }
 }
 
-// Exact recomputation of the queued samples (reference order, FP32).
+// Exact recomputation of the queued runs (reference order, FP32).  An entry
+// is (t << 40) | (mask << 32) | s0: samples s0 + k with bit k of the 4-bit mask
+// set.  A thread carries the four samples' sequential sums side by side: per 4
+// taps one 16-byte template load and 4 voltage loads feed 16 multiply-adds
+// (each sum still adds its products one at a time, in the reference's order).
 __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
-                             const float* __restrict__ bias, const unsigned long long* __restrict__ fix,
-                             uint32_t cap, const DevStatus* status, float* L)
+                             const float* __restrict__ Tp, const float* __restrict__ bias,
+                             const unsigned long long* __restrict__ fix, uint32_t cap, const DevStatus* status,
+                             float* L)
 {
     const uint32_t n = min(status->n_fix, cap);
+    const uint32_t W = d.W, Wp = (W + 3) & ~3u, W4 = W & ~3u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const unsigned long long e = fix[i];
-        const uint32_t t = (uint32_t)(e >> 32), s = (uint32_t)(e & 0xFFFFFFFFu);
-        L[(uint64_t)t * d.N + s] = exact_likelihood(d, V, T, bias[t], t, s);
+        const uint32_t t = (uint32_t)(e >> 40), mask = (uint32_t)(e >> 32) & 0xFu, s0 = (uint32_t)e;
+        const float b = bias[t];
+        if ((uint64_t)s0 + W + 3 > d.N) {   // the run reaches the end of the chunk: one sample at a time
+            for (uint32_t k = 0; k < 4; ++k)
+                if ((mask >> k) & 1u) L[(uint64_t)t * d.N + s0 + k] = exact_likelihood(d, V, T, b, t, s0 + k);
+            continue;
+        }
+        float a0 = b, a1 = b, a2 = b, a3 = b;
+        for (uint32_t c = 0; c < d.C; ++c) {
+            const float* vr = V + (uint64_t)c * d.N + s0;
+            const float* tr = Tp + ((uint64_t)t * d.C + c) * Wp;
+            float w0 = __ldg(vr), w1 = __ldg(vr + 1), w2 = __ldg(vr + 2);   // V[s0 + j + 0..2]
+            uint32_t j = 0;
+            for (; j < W4; j += 4) {
+                const float4 t4 = __ldg(reinterpret_cast<const float4*>(tr + j));
+                const float w3 = __ldg(vr + j + 3), w4 = __ldg(vr + j + 4), w5 = __ldg(vr + j + 5),
+                            w6 = __ldg(vr + j + 6);
+                a0 = __fadd_rn(a0, __fmul_rn(t4.x, w0)); a1 = __fadd_rn(a1, __fmul_rn(t4.x, w1));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.x, w2)); a3 = __fadd_rn(a3, __fmul_rn(t4.x, w3));
+                a0 = __fadd_rn(a0, __fmul_rn(t4.y, w1)); a1 = __fadd_rn(a1, __fmul_rn(t4.y, w2));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.y, w3)); a3 = __fadd_rn(a3, __fmul_rn(t4.y, w4));
+                a0 = __fadd_rn(a0, __fmul_rn(t4.z, w2)); a1 = __fadd_rn(a1, __fmul_rn(t4.z, w3));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.z, w4)); a3 = __fadd_rn(a3, __fmul_rn(t4.z, w5));
+                a0 = __fadd_rn(a0, __fmul_rn(t4.w, w3)); a1 = __fadd_rn(a1, __fmul_rn(t4.w, w4));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.w, w5)); a3 = __fadd_rn(a3, __fmul_rn(t4.w, w6));
+                w0 = w4; w1 = w5; w2 = w6;
+            }
+            for (; j < W; ++j) {   // remaining taps; w0..w2 hold V[s0 + j + 0..2]
+                const float tv = __ldg(tr + j);
+                const float w3 = __ldg(vr + j + 3);
+                a0 = __fadd_rn(a0, __fmul_rn(tv, w0)); a1 = __fadd_rn(a1, __fmul_rn(tv, w1));
+                a2 = __fadd_rn(a2, __fmul_rn(tv, w2)); a3 = __fadd_rn(a3, __fmul_rn(tv, w3));
+                w0 = w1; w1 = w2; w2 = w3;
+            }
+        }
+        float* Lr = L + (uint64_t)t * d.N + s0;
+        if (mask & 1u) Lr[0] = a0;
+        if (mask & 2u) Lr[1] = a1;
+        if (mask & 4u) Lr[2] = a2;
+        if (mask & 8u) Lr[3] = a3;
     }
 }
 
@@ -379,10 +433,18 @@ __global__ void voltage_repack_kernel(Dims d, const float* __restrict__ V, uint3
     }
 }
 
-// Tq[j][qp][h][n][e] = T[n][(2qp+h)*4+e][j]; tnorm[t][c] = |T[t][c][:]|.
+// Tq[j][qp][h][n][e] = T[n][(2qp+h)*4+e][j]; Tp[t][c][j] = T[t][c][j] (zero for
+// j >= W); tnorm[t][c] = |T[t][c][:]|.
 __global__ void template_pack_kernel(Dims d, const float* __restrict__ T, uint32_t Cq, uint32_t Np, float* Tq,
-                                     float* tnorm)
+                                     float* Tp, float* tnorm)
 {
+    const uint32_t Wp = (d.W + 3) & ~3u;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (uint64_t)d.M * d.C * Wp;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)(i % Wp);
+        const uint64_t tc = i / Wp;
+        Tp[i] = j < d.W ? T[tc * d.W + j] : 0.f;
+    }
     const uint64_t total = (uint64_t)d.W * Cq * Np * 4;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t e = i % 4;
@@ -446,7 +508,8 @@ int launch_tc_prepare_templates(const Dims& d, const Work& w, const float* T, cu
     if (!tc_config(d, &c)) return FBP_OK;
     const Layout& L = *w.lay;
     count_launch();
-    template_pack_kernel<<<256, 256, 0, st>>>(d, T, c.Cq, c.Np, w.at<float>(L.off_tt_hi), w.at<float>(L.off_tnorm));
+    template_pack_kernel<<<256, 256, 0, st>>>(d, T, c.Cq, c.Np, w.at<float>(L.off_tt_hi), w.at<float>(L.off_tpad),
+                                              w.at<float>(L.off_tnorm));
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }
@@ -487,6 +550,7 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     P.Tq = w.at<float>(L.off_tt_hi);
     P.bias = bias;
     P.tnorm = w.at<float>(L.off_tnorm);
+    P.Tp = w.at<float>(L.off_tpad);
     const bool all = nlist == d.nw;
     P.list = all ? nullptr : list;
     const uint64_t items = all ? ((uint64_t)d.N + kTile - 1) / kTile : nlist;
@@ -517,7 +581,7 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
         lik_tc_kernel<<<grid, kThreads, c.smem, st>>>(P);
     }
     KScope ks(&fbp_chunk_stats::ms_fixup, st);
-    fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, bias, P.fix, P.fix_cap, w.status(), Lk);
+    fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, P.Tp, bias, P.fix, P.fix_cap, w.status(), Lk);
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }
