@@ -122,6 +122,7 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
             L->screened = true;
             L->off_et = take(M * S2 * 8);
             L->off_xt = take(xt);
+            L->off_xtt = take(xt);                      // the same table transposed: XTT[f][t][b][a]
             uint64_t per = M * S2 * 4;
             uint64_t gb = (1ull << 30) / per;
             if (gb < 256) gb = 256;
@@ -132,6 +133,8 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
             L->off_mx = take(M * M * 4 + 2 * M * 4);   // max -X_ft per pair; max sqrt(E), max E per template
             L->cand_cap = 16ull << 20;                  // exact-scoring candidates per batch
             L->off_cand = take(L->cand_cap * 8);
+            // screening tables of each persistent screen CTA when they exceed shared memory
+            L->off_bscr = (M * S2 * 8 > 96 * 1024) ? take(296 * M * S2 * 8) : 0;
         }
     }
     L->bytes = align_up(off, 256);

@@ -47,12 +47,13 @@ __global__ void energy_table_kernel(Dims d, const float* __restrict__ T, float2*
     }
 }
 
-// Pair cross terms X_ft(a, b) for |a-b| <= W, one CTA per (f, t): products
+// Pair cross terms X_ft(a, b) for |a-b| <= W, one CTA per (f, t), stored as
+// XT[f][t][a][b] and transposed as XTT[f][t][b][a]: products
 // P_delta[u] = sum_c F[c,u] T[c,u+delta] in double, prefix sums over u, then
 // X_ft(a, b) = Q_delta[hi] - Q_delta[lo] with delta = a-b.
 constexpr int kLagChunk = 16;
 
-__global__ void __launch_bounds__(256) cross_table_kernel(Dims d, const float* __restrict__ T, float* XT,
+__global__ void __launch_bounds__(256) cross_table_kernel(Dims d, const float* __restrict__ T, float* XT, float* XTT,
                                                           float* max_negx)
 {
     typedef cub::BlockReduce<float, 256> RF;
@@ -94,6 +95,7 @@ __global__ void __launch_bounds__(256) cross_table_kernel(Dims d, const float* _
             const double v = hi > lo ? Q[li * (W + 1) + hi] - Q[li * (W + 1) + lo] : 0.0;
             const float xv = (float)v;
             XT[(((uint64_t)f * d.M + t) * S2 + a) * S2 + b] = xv;
+            XTT[(((uint64_t)f * d.M + t) * S2 + b) * S2 + a] = xv;
             mneg = fmaxf(mneg, -xv);
         }
         __syncthreads();
@@ -348,15 +350,17 @@ __device__ __forceinline__ uint32_t item_priority(uint64_t r, uint32_t WG, uint3
     return g * WG + br;
 }
 
-constexpr int kScrThreads = 256;
+constexpr int kScrThreads = 384;
 constexpr int kRowCap = 2048;   // surviving rows kept in shared memory
-constexpr int kCandCap = 1024;  // exact-scoring candidates per window
-constexpr int kRowUnroll = 8;   // items per lane whose loads are in flight together
-constexpr uint32_t kGStage = 48 * 1024;  // partial-correlation table staged in shared memory up to this size
+constexpr int kCandCap = 256;   // candidates buffered in shared memory per window (more go straight to the global list)
+constexpr int kScanQ = 8;       // items per lane of a row chunk (32 * kScanQ shifts)
+constexpr uint32_t kBStage = 96 * 1024;   // per-window item tables staged in shared memory up to this size
+constexpr uint32_t kScreenGrid = 148 * 2;  // persistent CTAs (two per SM); also sizes the unstaged table scratch
 
 struct ScreenShared {
     float lb;
     float nv;
+    float maxau2;
     unsigned long long best;
     uint32_t nA;
     uint32_t nrows;
@@ -364,21 +368,52 @@ struct ScreenShared {
     uint32_t gfull;   // the global candidate list ran out of room for this window
 };
 
+// Shared-memory bytes of screen_kernel for these sizes (tables staged or not).
+__host__ __device__ inline size_t screen_smem_bytes(uint32_t M, uint32_t S2, bool staged)
+{
+    const size_t s2p = (S2 + 3) & ~3u, mp = (M + 3) & ~3u;
+    size_t b = 5 * s2p * 4 + 2 * mp * 4 + (size_t)kRowCap * 8 + (size_t)kCandCap * 12;
+    b += (((size_t)S2 + 15) & ~(size_t)15) + (((size_t)M * S2 + 15) & ~(size_t)15);
+    if (staged) b += (size_t)M * S2 * 8;
+    return b + 64;
+}
+
+// One row of items seen from the lanes of a warp: the row's fixed part (uf,
+// lf), the per-item parts (ua[x], la[x]) and the cross terms xr[x] for x in
+// [lo, hi).  Item bounds: UB = (uf + ua[x]) - X, LB = (lf + la[x]) - X.
+struct ScreenRow {
+    float uf, lf;
+    const float* ua;
+    const float* la;
+    const float* xr;   // null: the templates share no channel, X == 0
+    int lo, hi;
+    uint32_t t, y;
+    bool fixed_a;
+};
+
 // Screening of one flagged window per CTA.
-//   rows, part 1: (a in A+, t) -- fixed a, the warp's lanes run over b;
-//   rows, part 2: (t, b) with L_t(b) > 0 -- fixed b, lanes run over a not in A+.
-// Phase B bounds every row from shared-memory quantities (each component at least
-// the item's, same monotone float order) and keeps the rows that can reach the
-// window's seed.  Phase C scans the kept rows: LB = max(est - bound) and per-row
-// maxima of est + bound.  Phase D lists the items of rows reaching max(LB, seed)
-// whose interval does; phase E scores them exactly, in parallel.
-__global__ void __launch_bounds__(kScrThreads) screen_kernel(
+//   rows, kind 1: (a in A+, t) -- a fixed, the lanes run over b (cross table XT[f][t][a][:]);
+//   rows, kind 2: (t, b) with L_t(b) > 0 -- b fixed, the lanes run over a not in A+
+//                 (transposed cross table XTT[f][t][b][:]).
+// Per window the CTA stages Bu/Bl[t][b] = G_t(b) +- beta_t(b) and Au/Al[a] =
+// G_f(a) +- alpha(a), with alpha + beta = K ((sqrt E_f(a) + sqrt E_t(b)) |v| +
+// E_f(a) + E_t(b)) the rigorous bound of |estimate - reference float value|
+// (K carries slack for the few float operations of this regrouping).  Phase B
+// bounds every row from shared-memory maxima (each component at least the
+// item's, same monotone float order) and keeps the rows that can reach the
+// window's seed; a quick lower bound from the best row of each warp prunes
+// them further.  Phase C scans the kept rows two at a time per warp (all
+// loads of both rows in flight together): LB = max(LB items) and per-row
+// maxima of UB.  Phase D lists the items of rows reaching max(LB, seed, 0)
+// whose UB does; score_kernel scores them exactly.
+__global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
     Dims d, const float* __restrict__ V, const float* __restrict__ T, const float* __restrict__ L,
     const float* __restrict__ theta, const float2* __restrict__ Etab, const float* __restrict__ XT,
-    const float* __restrict__ G, uint32_t k0, uint32_t kcount, const uint32_t* __restrict__ flag,
-    DevStatus* status, const uint32_t* __restrict__ best_lab, const uint32_t* __restrict__ best_idx,
-    const float* __restrict__ best_lik, unsigned long long* keys, const float* __restrict__ mx,
-    unsigned long long* gcand, uint32_t gcand_cap, const unsigned long long* __restrict__ chmask)
+    const float* __restrict__ XTT, const float* __restrict__ G, uint32_t k0, uint32_t kcount,
+    const uint32_t* __restrict__ flag, DevStatus* status, const uint32_t* __restrict__ best_lab,
+    const uint32_t* __restrict__ best_idx, const float* __restrict__ best_lik, unsigned long long* keys,
+    const float* __restrict__ mx, unsigned long long* gcand, uint32_t gcand_cap,
+    const unsigned long long* __restrict__ chmask, float* bscratch)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ ScreenShared sh;
@@ -390,32 +425,32 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
         typename SC::TempStorage sc;
     } tmp;
     const uint32_t S = d.S, W = d.W, M = d.M, S2 = 2 * S + 1;
+    const uint32_t s2p = (S2 + 3) & ~3u, mp = (M + 3) & ~3u;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kScrThreads / 32;
+    const bool staged = (uint64_t)M * S2 * 8 <= kBStage;
     // shared layout
-    float* gf = reinterpret_cast<float*>(smraw);          // [S2]   G_f(a)
-    float2* eft = reinterpret_cast<float2*>(gf + ((S2 + 3) & ~3u));  // [S2] (E_f(a), sqrt)
-    float* gmax = reinterpret_cast<float*>(eft + S2);     // [M] max_b G_t(b) in bounds
-    float* nx = gmax + M;                                  // [M] max -X_ft over items
-    float* ms = nx + M;                                    // [M] max_b sqrt(E_t(b))
-    float* me = ms + M;                                    // [M] max_b E_t(b)
-    float* vw = me + M;                                    // [C][W] window voltage
-    float* rowmax = vw + d.C * W;                          // [kRowCap]
-    uint32_t* rows = reinterpret_cast<uint32_t*>(rowmax + kRowCap);  // [kRowCap]
-    uint32_t* cand = rows + kRowCap;                       // [kCandCap][3]
-    uint32_t* alist = cand + 3 * kCandCap;                 // [S2]
-    uint8_t* fa = reinterpret_cast<uint8_t*>(alist + S2);  // [S2] bit0 in bounds, bit1 L_f > 0
-    uint8_t* pt = fa + ((S2 + 15) & ~15u);                 // [M][S2] L_t > 0
-    // [M][S2] staged G (if it fits), 16-byte aligned for vector stores
-    float* gst = reinterpret_cast<float*>(
-        smraw + ((static_cast<size_t>(pt + ((M * S2 + 15) & ~15u) - smraw) + 15) & ~static_cast<size_t>(15)));
-    const bool gstaged = (uint64_t)M * S2 * 4 <= kGStage;
+    float* Au = reinterpret_cast<float*>(smraw);   // [S2] G_f(a) + alpha(a), a in bounds
+    float* Al = Au + s2p;                          // [S2] G_f(a) - alpha(a)
+    float* Au2 = Al + s2p;                         // [S2] as Au for a in bounds and not in A+, else -inf
+    float* Al2 = Au2 + s2p;
+    uint32_t* alist = reinterpret_cast<uint32_t*>(Al2 + s2p);   // [S2] A+ in ascending order
+    float* gmaxu = reinterpret_cast<float*>(alist + s2p);       // [M] max_b Bu[t][b]
+    float* nx = gmaxu + mp;                                     // [M] max -X_ft over items
+    float* rowmax = nx + mp;                                    // [kRowCap]
+    uint32_t* rows = reinterpret_cast<uint32_t*>(rowmax + kRowCap);   // [kRowCap]
+    uint32_t* cand = rows + kRowCap;                            // [kCandCap][3]
+    uint8_t* fa = reinterpret_cast<uint8_t*>(cand + 3 * kCandCap);   // [S2] bit0 in bounds, bit1 L_f > 0
+    uint8_t* pt = fa + ((S2 + 15) & ~15u);                      // [M][S2] L_t(b) > 0, b in bounds
+    float* Bu = staged ? reinterpret_cast<float*>(pt + ((M * S2 + 15) & ~15u))
+                       : bscratch + (uint64_t)blockIdx.x * M * S2 * 2;   // [M][S2]
+    float* Bl = Bu + (size_t)M * S2;                                        // [M][S2]
     const uint64_t items = (uint64_t)S2 * S2 * M;
     const uint64_t nloc = (items - 1) / d.WG + 1;
     const uint64_t slots = nloc * d.WG;
     uint32_t lbits = 0;
     while ((1u << lbits) < d.WG) ++lbits;
     const float u = 1.0f / 16777216.0f;
-    const float K = 1.01f * 1.05f * u * 2.0f * ((float)d.C * W + d.C + W + 8);
+    const float K = 1.01f * 1.05f * u * 2.0f * ((float)d.C * W + d.C + W + 24);
     const uint32_t nflag = status->n_flag;
     unsigned long long exact_n = 0, item_n = 0;
     for (uint32_t kk = blockIdx.x; kk < kcount; kk += gridDim.x) {
@@ -427,58 +462,68 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
         const float seed = best_lik[id];
         const float thr0 = fmaxf(seed, 0.f);
         const float* Gk = G + (uint64_t)kk * M * S2;
+        const unsigned long long mf = chmask[f];
         __syncthreads();
         // ---- phase A: window quantities
         float nv2 = 0.f;
         for (uint32_t e = threadIdx.x; e < d.C * W; e += blockDim.x) {
             const uint32_t c = e / W, j = e - c * W;
             const float v = V[(uint64_t)c * d.N + p + j];
-            vw[e] = v;
             nv2 = fmaf(v, v, nv2);
         }
         for (uint32_t x = threadIdx.x; x < S2; x += blockDim.x) {
             const uint64_t xp = (uint64_t)x + p;
             const bool inb = xp >= S && xp < (uint64_t)d.N - W + S;
             fa[x] = inb ? ((L[(uint64_t)f * d.N + xp - S] > 0.f) ? 3 : 1) : 0;
-            gf[x] = Gk[(uint64_t)f * S2 + x];
-            eft[x] = Etab[(uint64_t)f * S2 + x];
         }
-        if (gstaged) {
-            if (((M * S2) & 3u) == 0 && ((reinterpret_cast<uintptr_t>(Gk) & 15u) == 0)) {
-                const float4* g4 = reinterpret_cast<const float4*>(Gk);
-                float4* s4 = reinterpret_cast<float4*>(gst);
+        for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) nx[t] = mx[(uint64_t)f * M + t];
+        const float nvs = RF(tmp.rf).Sum(nv2);
+        if (threadIdx.x == 0) {
+            sh.nv = sqrtf(nvs) * 1.001f;
+            sh.best = 0ull;
+            sh.nrows = 0;
+            sh.ncand = 0;
+            sh.gfull = 0;
+        }
+        __syncthreads();
+        const float nv = sh.nv;
+        float ma2 = -INFINITY;
+        for (uint32_t x = threadIdx.x; x < S2; x += blockDim.x) {
+            const float2 ea = Etab[(uint64_t)f * S2 + x];
+            const float al = K * fmaf(nv, ea.y, ea.x);
+            const float g = Gk[(uint64_t)f * S2 + x];
+            const uint8_t fl = fa[x];
+            const float au = (fl & 1) ? g + al : -INFINITY, alo = (fl & 1) ? g - al : -INFINITY;
+            Au[x] = au;
+            Al[x] = alo;
+            Au2[x] = fl == 1 ? au : -INFINITY;
+            Al2[x] = fl == 1 ? alo : -INFINITY;
+            if (fl == 1) ma2 = fmaxf(ma2, au);
+        }
 #pragma unroll 4
-                for (uint32_t e = threadIdx.x; e < M * S2 / 4; e += blockDim.x) s4[e] = g4[e];
-            } else {
-#pragma unroll 8
-                for (uint32_t e = threadIdx.x; e < M * S2; e += blockDim.x) gst[e] = Gk[e];
-            }
-        }
-#pragma unroll 8
         for (uint32_t e = threadIdx.x; e < M * S2; e += blockDim.x) {
             const uint32_t t = e / S2, x = e - t * S2;
             const uint64_t xp = (uint64_t)x + p;
             const bool inb = xp >= S && xp < (uint64_t)d.N - W + S;
+            const float2 eb = Etab[e];
+            const float be = K * fmaf(nv, eb.y, eb.x);
+            const float g = Gk[e];
+            Bu[e] = inb ? g + be : -INFINITY;
+            Bl[e] = inb ? g - be : -INFINITY;
             pt[e] = (inb && L[(uint64_t)t * d.N + xp - S] > 0.f) ? 1 : 0;
         }
-        for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
-            nx[t] = mx[(uint64_t)f * M + t];
-            ms[t] = mx[(uint64_t)M * M + t];
-            me[t] = mx[(uint64_t)M * M + M + t];
+        {
+            const float m2 = RF(tmp.rf).Reduce(ma2, cub::Max());
+            if (threadIdx.x == 0) sh.maxau2 = m2;
         }
+        __syncthreads();   // Bu/Bl (global scratch too: the block's own writes) visible
         for (uint32_t t = warp; t < M; t += nwarps) {
             float m = -INFINITY;
-            for (uint32_t x = lane; x < S2; x += 32) {
-                const uint64_t xp = (uint64_t)x + p;
-                if (xp >= S && xp < (uint64_t)d.N - W + S) m = fmaxf(m, Gk[(uint64_t)t * S2 + x]);
-            }
+            for (uint32_t x = lane; x < S2; x += 32) m = fmaxf(m, Bu[(uint64_t)t * S2 + x]);
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-            if (lane == 0) gmax[t] = m;
+            if (lane == 0) gmaxu[t] = m;
         }
-        const float nvs = RF(tmp.rf).Sum(nv2);
-        if (threadIdx.x == 0) { sh.nv = sqrtf(nvs) * 1.001f; sh.best = 0ull; sh.nrows = 0; sh.ncand = 0; sh.gfull = 0; }
-        __syncthreads();
         // A+ list in ascending order
         {
             uint32_t base = 0;
@@ -495,98 +540,100 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
         }
         __syncthreads();
         const uint32_t nA = sh.nA;
-        const float nv = sh.nv;
+        const float maxau2 = sh.maxau2;
         const uint32_t rows1 = nA * M, rows_all = rows1 + M * S2;
-        // ---- phase B: row bounds, keep rows that can reach the seed
-        bool overflow = false;
-        for (uint32_t r = threadIdx.x; r < rows_all; r += blockDim.x) {
-            float ub;
+        // row r -> bound of every item in it (phase B), and its scan description
+        auto row_bound = [&](uint32_t r) -> float {
+            if (r < rows1) {
+                const uint32_t t = r % M;
+                return (Au[alist[r / M]] + gmaxu[t]) + nx[t];
+            }
+            const uint32_t e = r - rows1;
+            if (!pt[e]) return -INFINITY;
+            return (Bu[e] + maxau2) + nx[e / S2];
+        };
+        auto describe = [&](uint32_t r, ScreenRow& R) {
             if (r < rows1) {
                 const uint32_t a = alist[r / M], t = r % M;
-                const float2 ea = eft[a];
-                ub = gf[a] + gmax[t] + nx[t] + K * ((ea.y + ms[t]) * nv + ea.x + me[t]);
+                R.fixed_a = true;
+                R.t = t;
+                R.y = a;
+                R.uf = Au[a];
+                R.lf = Al[a];
+                R.ua = Bu + (size_t)t * S2;
+                R.la = Bl + (size_t)t * S2;
+                R.xr = (mf & chmask[t]) ? XT + (((uint64_t)f * M + t) * S2 + a) * S2 : nullptr;
             } else {
-                const uint32_t e = r - rows1;
-                if (!pt[e]) continue;
-                const uint32_t t = e / S2, b = e - t * S2;
-                const float2 eb = Etab[(uint64_t)t * S2 + b];
-                ub = gmax[f] + Gk[(uint64_t)t * S2 + b] + nx[t] + K * ((ms[f] + eb.y) * nv + me[f] + eb.x);
+                const uint32_t e = r - rows1, t = e / S2, b = e - t * S2;
+                R.fixed_a = false;
+                R.t = t;
+                R.y = b;
+                R.uf = Bu[e];
+                R.lf = Bl[e];
+                R.ua = Au2;
+                R.la = Al2;
+                R.xr = (mf & chmask[t]) ? XTT + (((uint64_t)f * M + t) * S2 + b) * S2 : nullptr;
             }
-            if (ub < thr0) continue;
+            R.lo = max(0, (int)R.y - (int)W);
+            R.hi = min((int)S2, (int)R.y + (int)W + 1);
+        };
+        // scan of up to two rows by one warp: cross terms of both rows loaded
+        // together, then (listing == false) LB/UB maxima, or (listing) candidates
+        auto scan2 = [&](const ScreenRow (&R)[2], bool listing, float thr, float (&lbm)[2], float (&ubm)[2]) {
+            const int span = max(R[0].hi - R[0].lo, R[1].hi - R[1].lo);
+            for (int c0 = 0; c0 < span; c0 += 32 * kScanQ) {
+                float xv[2][kScanQ];
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int q = 0; q < kScanQ; ++q) {
+                        const int x = R[i].lo + c0 + (int)lane + 32 * q;
+                        xv[i][q] = (x < R[i].hi && R[i].xr) ? __ldg(R[i].xr + x) : 0.f;
+                    }
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+#pragma unroll
+                    for (int q = 0; q < kScanQ; ++q) {
+                        const int x = R[i].lo + c0 + (int)lane + 32 * q;
+                        if (x >= R[i].hi) continue;
+                        const float ub = (R[i].uf + R[i].ua[x]) - xv[i][q];
+                        if (!listing) {
+                            const float lb = (R[i].lf + R[i].la[x]) - xv[i][q];
+                            lbm[i] = fmaxf(lbm[i], lb);
+                            ubm[i] = fmaxf(ubm[i], ub);
+                            continue;
+                        }
+                        if (!(ub >= thr)) continue;
+                        const uint32_t a = R[i].fixed_a ? R[i].y : (uint32_t)x;
+                        const uint32_t b = R[i].fixed_a ? (uint32_t)x : R[i].y;
+                        const uint32_t slot = atomicAdd(&sh.ncand, 1u);
+                        if (slot < (uint32_t)kCandCap) {
+                            cand[3 * slot] = a;
+                            cand[3 * slot + 1] = R[i].t;
+                            cand[3 * slot + 2] = b;
+                        } else {
+                            const uint32_t g = atomicAdd(&status->cand_count, 1u);
+                            if (g < gcand_cap)
+                                gcand[g] = ((unsigned long long)kk << 32) | ((unsigned long long)R[i].t << 20) |
+                                           ((unsigned long long)a << 10) | (unsigned long long)b;
+                            else
+                                sh.gfull = 1;
+                        }
+                    }
+                }
+            }
+        };
+        // ---- phase B: row bounds, keep rows that can reach the seed
+        for (uint32_t r = threadIdx.x; r < rows_all; r += blockDim.x) {
+            const float ub = row_bound(r);
+            if (!(ub >= thr0)) continue;
             const uint32_t slot = atomicAdd(&sh.nrows, 1u);
             if (slot < (uint32_t)kRowCap) { rows[slot] = r; rowmax[slot] = ub; }
         }
         __syncthreads();
         uint32_t nrows = sh.nrows;
-        if (nrows > (uint32_t)kRowCap) { overflow = true; nrows = rows_all; }
-        // row scan: (a fixed, lanes over b) or (t, b fixed, lanes over a); every
-        // load of the lane's items is issued before any arithmetic
-        auto row_items = [&](uint32_t r, float thr, bool listing, float& lbm, float& ubm) {
-            uint32_t a0 = 0, t, b0 = 0;
-            bool fixed_a;
-            if (r < rows1) {
-                a0 = alist[r / M];
-                t = r % M;
-                fixed_a = true;
-            } else {
-                const uint32_t e = r - rows1;
-                if (!pt[e]) return;
-                t = e / S2;
-                b0 = e - t * S2;
-                fixed_a = false;
-            }
-            const float* xt_ft = XT + ((uint64_t)f * M + t) * S2 * S2;
-            const bool cross = (chmask[f] & chmask[t]) != 0ull;   // disjoint channels: X_ft == 0
-            const float* gt = (gstaged ? gst : Gk) + (uint64_t)t * S2;
-            const float2* et = Etab + (uint64_t)t * S2;
-            for (uint32_t x0 = 0; x0 < S2; x0 += 32 * kRowUnroll) {
-                bool ok[kRowUnroll];
-                float g2[kRowUnroll], xv[kRowUnroll];
-                float2 e2[kRowUnroll];
-#pragma unroll
-                for (int q = 0; q < kRowUnroll; ++q) {
-                    const uint32_t x = x0 + lane + 32 * q;
-                    const uint32_t a = fixed_a ? a0 : x, b = fixed_a ? x : b0;
-                    bool v = x < S2;
-                    if (v) v = fixed_a ? (fa[b] & 1) != 0 : fa[a] == 1;
-                    v = v && (a > b ? a - b : b - a) <= W;
-                    ok[q] = v;
-                    g2[q] = v ? gt[b] : 0.f;
-                    e2[q] = make_float2(v ? reinterpret_cast<const float*>(et)[2 * b] : 0.f, 0.f);
-                    xv[q] = (v && cross) ? xt_ft[(uint64_t)a * S2 + b] : 0.f;
-                }
-#pragma unroll
-                for (int q = 0; q < kRowUnroll; ++q) {
-                    if (!ok[q]) continue;
-                    const uint32_t x = x0 + lane + 32 * q;
-                    const uint32_t a = fixed_a ? a0 : x, b = fixed_a ? x : b0;
-                    const float2 ea = eft[a];
-                    const float est = gf[a] + g2[q] - xv[q];
-                    const float sb = __fsqrt_ru(e2[q].x);   // rounded up: the bound stays an upper bound
-                    const float bound = K * ((ea.y + sb) * nv + ea.x + e2[q].x);
-                    if (!listing) {
-                        lbm = fmaxf(lbm, est - bound);
-                        ubm = fmaxf(ubm, est + bound);
-                        ++item_n;
-                        continue;
-                    }
-                    if (est + bound < thr) continue;
-                    const uint32_t slot = atomicAdd(&sh.ncand, 1u);
-                    if (slot < (uint32_t)kCandCap) {
-                        cand[3 * slot] = a;
-                        cand[3 * slot + 1] = t;
-                        cand[3 * slot + 2] = b;
-                    } else {
-                        const uint32_t g = atomicAdd(&status->cand_count, 1u);
-                        if (g < gcand_cap)
-                            gcand[g] = ((unsigned long long)kk << 32) | ((unsigned long long)t << 20) |
-                                       ((unsigned long long)a << 10) | (unsigned long long)b;
-                        else
-                            sh.gfull = 1;
-                    }
-                }
-            }
-        };
+        const bool overflow = nrows > (uint32_t)kRowCap;
+        if (overflow) nrows = rows_all;
         // ---- phase B2: a quick lower bound from the highest-bound row of each
         // warp's share, then keep only rows whose bound reaches it
         float lb = -INFINITY;
@@ -602,9 +649,12 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
                 if (ou > bu || (ou == bu && oi < bi)) { bu = ou; bi = oi; }
             }
             if (bi != 0xFFFFFFFFu) {
-                float lbm = -INFINITY, ubm = -INFINITY;
-                row_items(rows[bi], thr0, false, lbm, ubm);
-                lb = lbm;
+                ScreenRow R[2];
+                describe(rows[bi], R[0]);
+                R[1].lo = R[1].hi = 0;
+                float lbm[2] = {-INFINITY, -INFINITY}, ubm[2] = {-INFINITY, -INFINITY};
+                scan2(R, false, 0.f, lbm, ubm);
+                lb = lbm[0];
             }
         }
         {
@@ -629,25 +679,52 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
                 nrows = base;
             }
         }
-        // ---- phase C: lower bound and per-row upper bounds
-        for (uint32_t i = warp; i < nrows; i += nwarps) {
+        // a kept row (or, after an overflow, any row whose bound reaches thr),
+        // else an empty range
+        auto describe_kept = [&](uint32_t i, float thr, bool use_rowmax, ScreenRow& R) {
+            R.lo = R.hi = 0;
+            if (i >= nrows) return;
             const uint32_t r = overflow ? i : rows[i];
-            float lbm = -INFINITY, ubm = -INFINITY;
-            row_items(r, thr0, false, lbm, ubm);
+            if (overflow ? !(row_bound(r) >= thr) : (use_rowmax && !(rowmax[i] >= thr))) return;
+            describe(r, R);
+        };
+        // ---- phase C: lower bound and per-row upper bounds, two rows per warp at a time
+        {
+            uint64_t scanned = 0;
+            for (uint32_t i = 2 * warp; i < nrows; i += 2 * nwarps) {
+                ScreenRow R[2];
+                describe_kept(i, thr0, false, R[0]);
+                describe_kept(i + 1, thr0, false, R[1]);
+                scanned += (uint64_t)(R[0].hi - R[0].lo) + (uint64_t)(R[1].hi - R[1].lo);
+                float lbm[2] = {-INFINITY, -INFINITY}, ubm[2] = {-INFINITY, -INFINITY};
+                scan2(R, false, 0.f, lbm, ubm);
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) ubm = fmaxf(ubm, __shfl_xor_sync(0xffffffffu, ubm, off));
-            if (!overflow && lane == 0) rowmax[i] = ubm;
-            lb = fmaxf(lb, lbm);
+                for (int q = 0; q < 2; ++q) {
+                    float m = ubm[q];
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+                    ubm[q] = m;
+                    lb = fmaxf(lb, lbm[q]);
+                }
+                if (!overflow && lane == 0) {
+                    rowmax[i] = ubm[0];
+                    if (i + 1 < nrows) rowmax[i + 1] = ubm[1];
+                }
+            }
+            if (lane == 0) item_n += scanned;
         }
         const float lbs = RF(tmp.rf).Reduce(lb, cub::Max());
         if (threadIdx.x == 0) sh.lb = lbs;
         __syncthreads();
         const float thr = fmaxf(fmaxf(sh.lb, seed), 0.f);
-        // ---- phase D: candidate list
-        for (uint32_t i = warp; i < nrows; i += nwarps) {
-            if (!overflow && rowmax[i] < thr) continue;
-            float lbm, ubm;
-            row_items(overflow ? i : rows[i], thr, true, lbm, ubm);
+        // ---- phase D: candidate list from the rows reaching thr, two per warp at a time
+        for (uint32_t i = 2 * warp; i < nrows; i += 2 * nwarps) {
+            ScreenRow R[2];
+            describe_kept(i, thr, true, R[0]);
+            describe_kept(i + 1, thr, true, R[1]);
+            if (R[0].hi == R[0].lo && R[1].hi == R[1].lo) continue;
+            float lbm[2], ubm[2];
+            scan2(R, true, thr, lbm, ubm);
         }
         __syncthreads();
         const uint32_t ncand = sh.ncand;
@@ -671,22 +748,18 @@ __global__ void __launch_bounds__(kScrThreads) screen_kernel(
                 gcand[i] = ~0ull;
             for (uint32_t i = threadIdx.x; i < nrows; i += blockDim.x) {
                 const uint32_t r = overflow ? i : rows[i];
-                uint32_t a = 0, t, b = 0;
-                bool fixed_a;
-                if (r < rows1) { a = alist[r / M]; t = r % M; fixed_a = true; }
-                else { const uint32_t e = r - rows1; if (!pt[e]) continue; t = e / S2; b = e - t * S2; fixed_a = false; }
-                for (uint32_t x = 0; x < S2; ++x) {
-                    if (fixed_a) { b = x; if (!(fa[b] & 1)) continue; } else { a = x; if (fa[a] != 1) continue; }
-                    if ((a > b ? a - b : b - a) > W) continue;
-                    const float2 ea = eft[a], eb = Etab[(uint64_t)t * S2 + b];
-                    const float est = gf[a] + Gk[(uint64_t)t * S2 + b] -
-                                      XT[(((uint64_t)f * M + t) * S2 + a) * S2 + b];
-                    const float bound = K * ((ea.y + eb.y) * nv + ea.x + eb.x);
-                    if (est + bound < thr) continue;
-                    const float v = pair_exact_g(d, T, V, f, t, p, a, b);
+                if (!(row_bound(r) >= thr)) continue;
+                ScreenRow R;
+                describe(r, R);
+                for (int x = R.lo; x < R.hi; ++x) {
+                    const float xv = R.xr ? R.xr[x] : 0.f;
+                    const float ub = (R.uf + R.ua[x]) - xv;
+                    if (!(ub >= thr)) continue;
+                    const uint32_t a = R.fixed_a ? R.y : (uint32_t)x, b = R.fixed_a ? (uint32_t)x : R.y;
+                    const float v = pair_exact_g(d, T, V, f, R.t, p, a, b);
                     ++exact_n;
                     if (!(v > 0.f)) continue;
-                    const uint64_t rr0 = (uint64_t)t + (uint64_t)M * a + (uint64_t)M * S2 * b;
+                    const uint64_t rr0 = (uint64_t)R.t + (uint64_t)M * a + (uint64_t)M * S2 * b;
                     uint32_t pr = item_priority(rr0, d.WG, lbits);
                     for (uint64_t rr = rr0 + items; rr < slots; rr += items) {
                         const uint32_t p2 = item_priority(rr, d.WG, lbits);
@@ -775,7 +848,8 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     const size_t smem = (size_t)2 * d.C * d.W * 4 + 8 + (size_t)kLagChunk * (d.W + 1) * 8;
     if (smem > 200 * 1024) return fail(FBP_E_ARG, "template too large for the pair table kernel");
     FBP_CUDA(cudaFuncSetAttribute(cross_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    cross_table_kernel<<<d.M * d.M, 256, smem, st>>>(d, T, w.at<float>(L.off_xt), w.at<float>(L.off_mx));
+    cross_table_kernel<<<d.M * d.M, 256, smem, st>>>(d, T, w.at<float>(L.off_xt), w.at<float>(L.off_xtt),
+                                                     w.at<float>(L.off_mx));
     energy_max_kernel<<<(d.M + 127) / 128, 128, 0, st>>>(d, w.at<float2>(L.off_et), w.at<float>(L.off_mx) + (size_t)d.M * d.M);
     template_order_kernel<<<1, 256, d.M * 4, st>>>(d, T, w.at<uint32_t>(L.off_perm),
                                                   reinterpret_cast<unsigned long long*>(w.at<uint32_t>(L.off_perm) + ((d.M + 1) & ~1u)));
@@ -823,10 +897,8 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     const size_t smem_a = pc.smem;
     if (Q == 0) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     const uint32_t pc_threads = 32u * std::min<uint32_t>((S2 + 15) / 16, kPcMaxWarps);
-    const size_t gstage = (size_t)d.M * S2 * 4 <= 48 * 1024 ? (size_t)d.M * S2 * 4 : 0;
-    const size_t smem_b = (((size_t)S2 + 3) & ~(size_t)3) * 4 + (size_t)S2 * 8 + (size_t)4 * d.M * 4 +
-                          (size_t)d.C * d.W * 4 + (size_t)kRowCap * 8 + (size_t)kCandCap * 12 + (size_t)S2 * 4 +
-                          (((size_t)S2 + 15) & ~(size_t)15) + (((size_t)d.M * S2 + 15) & ~(size_t)15) + gstage + 80;
+    const bool bstaged = (uint64_t)d.M * S2 * 8 <= kBStage;
+    const size_t smem_b = screen_smem_bytes(d.M, S2, bstaged);
     if (smem_b > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
     FBP_CUDA(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
     const uint32_t groups = (d.M + Q - 1) / Q;
@@ -862,14 +934,15 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
         }
 #undef FBP_PC
         }
-        const uint32_t gb = kc < 148u * 8 ? kc : 148u * 8;
+        const uint32_t gb = kc < kScreenGrid ? kc : kScreenGrid;
         FBP_CUDA(cudaMemsetAsync(&w.status()->cand_count, 0, 4, st));
         unsigned long long* gcand = w.at<unsigned long long>(L.off_cand);
         {
         KScope ks(&fbp_chunk_stats::ms_screen, st);
-        screen_kernel<<<gb, kScrThreads, smem_b, st>>>(d, V, T, w.L(), theta, Et, XT, G, k0, kc, w.flag(), w.status(),
-                                                       w.best_lab(), w.best_idx(), w.best_lik(), w.keys(),
-                                                       w.at<float>(L.off_mx), gcand, (uint32_t)L.cand_cap, chm);
+        screen_kernel<<<gb, kScrThreads, smem_b, st>>>(d, V, T, w.L(), theta, Et, XT, w.at<float>(L.off_xtt), G, k0, kc,
+                                                       w.flag(), w.status(), w.best_lab(), w.best_idx(), w.best_lik(),
+                                                       w.keys(), w.at<float>(L.off_mx), gcand, (uint32_t)L.cand_cap, chm,
+                                                       bstaged ? nullptr : w.at<float>(L.off_bscr));
         }
         KScope ks(&fbp_chunk_stats::ms_score, st);
         score_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, w.flag(), k0, w.best_lab(), w.best_idx(), gcand,
