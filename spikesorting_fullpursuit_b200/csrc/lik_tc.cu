@@ -32,6 +32,8 @@
 // draining its own operations.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include "fbp_internal.cuh"
 
 namespace fbp {
@@ -140,7 +142,7 @@ struct TcParams {
     const uint32_t* list; // listed windows (mode 1) or null (mode 0: contiguous tiles)
     uint32_t nitems;      // tiles (mode 0) or listed windows (mode 1)
     uint32_t rows;        // rows of each Vq channel block
-    uint32_t Cq, Np, ntiles, R8, stages, ncols;
+    uint32_t Cq, Np, ntiles, R8, stages, ncols, group;   // group: k-steps per template stage
     float* L;
     unsigned long long* fix;
     uint32_t fix_cap;
@@ -167,7 +169,8 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t strip_bytes = P.R8 * 16;                  // one 4-channel block of a tile strip
     const uint32_t tile_bytes = P.Cq * strip_bytes;
-    const uint32_t stage_bytes = P.Np * 32;                  // one (tap, channel pair) of templates
+    const uint32_t kstep_bytes = P.Np * 32;                  // one (tap, channel pair) of templates
+    const uint32_t stage_bytes = P.group * kstep_bytes;      // P.group consecutive k-steps per bulk copy
     unsigned char* A = smem;
     unsigned char* B = A + P.ntiles * tile_bytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(B + P.stages * stage_bytes);
@@ -184,6 +187,7 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
     float* sbias = bnd + P.ntiles * d.M;                          // [M]
 
     const uint32_t ksteps = d.W * (P.Cq / 2);
+    const uint32_t ngroups = (ksteps + P.group - 1) / P.group;
     if (threadIdx.x == 0) {
         mbar_init(a_full, 1);
         mbar_init(acc_full, 1);
@@ -225,12 +229,13 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
                 for (uint32_t q = 0; q < P.Cq; ++q)
                     bulk_g2s(A + i * tile_bytes + q * strip_bytes,
                              P.Vq + ((uint64_t)q * P.rows + t_s0[i]) * 4, strip_bytes, a_full);
-            // templates, one stage per (tap, channel pair)
-            for (uint32_t k = 0; k < ksteps; ++k) {
-                const uint32_t st = k % P.stages, round = k / P.stages;
+            // templates, one stage per P.group consecutive (tap, channel pair) steps
+            for (uint32_t g = 0; g < ngroups; ++g) {
+                const uint32_t st = g % P.stages, round = g / P.stages;
                 if (round > 0 && !mbar_wait(&b_empty[st], (round - 1) & 1)) { atomicOr(err, 1u); break; }
-                mbar_expect_tx(&b_full[st], stage_bytes);
-                bulk_g2s(B + st * stage_bytes, P.Tq + (uint64_t)k * P.Np * 8, stage_bytes, &b_full[st]);
+                const uint32_t k0 = g * P.group, nk = min(P.group, ksteps - k0);
+                mbar_expect_tx(&b_full[st], nk * kstep_bytes);
+                bulk_g2s(B + st * stage_bytes, P.Tq + (uint64_t)k0 * P.Np * 8, nk * kstep_bytes, &b_full[st]);
             }
         }
     } else if (warp == 1) {
@@ -239,16 +244,20 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
             bool ok = mbar_wait(a_full, 0);
             const uint32_t a_base = smem_u32(A), b_base = smem_u32(B);
             uint32_t issued = 0;
-            for (uint32_t k = 0; ok && k < ksteps; ++k) {
-                const uint32_t st = k % P.stages, round = k / P.stages;
+            for (uint32_t g = 0; ok && g < ngroups; ++g) {
+                const uint32_t st = g % P.stages, round = g / P.stages;
                 if (!mbar_wait(&b_full[st], round & 1)) { ok = false; break; }
                 tc_fence_after();
-                const uint32_t j = k / (P.Cq / 2), qp = k % (P.Cq / 2);
-                const uint64_t bdesc = umma_desc(b_base + st * stage_bytes, P.Np * 16, 128);
-                for (uint32_t i = 0; i < P.ntiles; ++i) {
-                    const uint32_t a_addr = a_base + i * tile_bytes + (2 * qp) * strip_bytes + j * 16;
-                    const uint64_t adesc = umma_desc(a_addr, strip_bytes, 128);
-                    umma_tf32(tmem + i * P.Np, adesc, bdesc, idesc, k > 0 ? 1u : 0u);
+                const uint32_t k0 = g * P.group, nk = min(P.group, ksteps - k0);
+                for (uint32_t kq = 0; kq < nk; ++kq) {
+                    const uint32_t k = k0 + kq;
+                    const uint32_t j = k / (P.Cq / 2), qp = k % (P.Cq / 2);
+                    const uint64_t bdesc = umma_desc(b_base + st * stage_bytes + kq * kstep_bytes, P.Np * 16, 128);
+                    for (uint32_t i = 0; i < P.ntiles; ++i) {
+                        const uint32_t a_addr = a_base + i * tile_bytes + (2 * qp) * strip_bytes + j * 16;
+                        const uint64_t adesc = umma_desc(a_addr, strip_bytes, 128);
+                        umma_tf32(tmem + i * P.Np, adesc, bdesc, idesc, k > 0 ? 1u : 0u);
+                    }
                 }
                 umma_commit(&b_empty[st]);
                 ++issued;
@@ -463,7 +472,7 @@ __global__ void template_pack_kernel(Dims d, const float* __restrict__ T, uint32
 }
 
 struct TcConfig {
-    uint32_t Cq, Np, ntiles, R8, stages, ncols;
+    uint32_t Cq, Np, ntiles, R8, stages, ncols, group;
     size_t smem;
 };
 
@@ -483,10 +492,11 @@ bool tc_config(const Dims& d, TcConfig* c)
         c->ncols = 32;
         while (c->ncols < cols) c->ncols <<= 1;
         const size_t strips = (size_t)c->ntiles * c->Cq * c->R8 * 16;
-        const size_t stage = (size_t)c->Np * 32;
-        c->stages = 8;
-        while (c->stages > 2 && strips + c->stages * stage > 160 * 1024) c->stages >>= 1;
-        c->smem = strips + c->stages * stage + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
+        // template stages of about 12 KB (whole k-steps), three in the ring
+        c->group = (uint32_t)std::max<size_t>(1, (12 * 1024) / ((size_t)c->Np * 32));
+        c->stages = 3;
+        while (c->group > 1 && strips + c->stages * c->group * (size_t)c->Np * 32 > 160 * 1024) c->group >>= 1;
+        c->smem = strips + c->stages * (size_t)c->group * c->Np * 32 + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
                   (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + 1024;
         if (c->smem <= 200 * 1024) return true;
         if (c->ntiles == 1) return false;
@@ -562,6 +572,7 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     P.R8 = c.R8;
     P.stages = c.stages;
     P.ncols = c.ncols;
+    P.group = c.group;
     P.L = Lk;
     P.fix = w.at<unsigned long long>(L.off_fix);
     P.fix_cap = (uint32_t)L.n_fix_cap;
