@@ -286,7 +286,7 @@ def main():
     listed, flagged = st_stage["listed"], st_stage["flagged"]
     fam = {
         "lik_tc_kernel": (st_stage["ms_lik_tc"], "tensor", 2.0 * M * C * W * W * listed),
-        "fixup_kernel": (st_stage["ms_fixup"], "fp32", 2.0 * C * W * st_stage["fixups"]),
+        "fixup_kernel": (st_stage["ms_fixup"], "fp32", 2.0 * C * W * 4 * st_stage["fixup_runs_queued"]),
         "partial_corr_kernel": (st_stage["ms_partial_corr"], "fp32", 2.0 * M * C * W * S2 * flagged),
         "screen_kernel": (st_stage["ms_screen"], "hbm", (4.0 * C * W + 8.0 * M * S2 + 4.0 * M * S2) * flagged),
         "score_kernel": (st_stage["ms_score"], "fp32", 5.0 * C * W * st_stage["pair_exact"]),
@@ -331,7 +331,7 @@ def main():
             "gpu_launches": launches,
             "stages_ms": {k[3:]: v for k, v in st_stage.items() if k.startswith("ms_") and v > 0},
             "kernels": kernels,
-            "stats": {k: st_stage[k] for k in ("passes", "n_spikes", "listed", "flagged", "fixups", "pair_exact")},
+            "stats": {k: st_stage[k] for k in ("passes", "n_spikes", "listed", "flagged", "fixups", "fixup_runs_queued", "pair_exact")},
             "roofline": roof,
             "plain_fp32": plain,
             "cpu_baseline": cpu,

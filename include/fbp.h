@@ -56,7 +56,8 @@ typedef struct fbp_chunk_stats {
     uint32_t n_spikes;       /* spikes written */
     uint64_t listed;         /* windows whose likelihood was (re)computed, summed over passes */
     uint64_t flagged;        /* windows given to the overlap recheck, summed over passes */
-    uint64_t fixups;         /* likelihood samples recomputed exactly after the tensor-core pass */
+    uint64_t fixups;         /* likelihood samples recomputed exactly after the tensor-core product
+                                (4 per queued run of consecutive samples) */
     uint64_t pair_exact;     /* overlap items whose pair likelihood was computed exactly */
     float ms_likelihood;     /* device time per stage, summed over passes (0 unless timing) */
     float ms_argmax;
@@ -72,7 +73,8 @@ typedef struct fbp_chunk_stats {
     float ms_screen;         /* screening of the recheck items */
     float ms_score;          /* exact scoring of the recheck candidates */
     float ms_overlap_plain;  /* brute-force recheck */
-    uint32_t pad0;
+    uint32_t fixup_runs_queued; /* runs recomputed by the separate fixup kernel (the others inside
+                                   the likelihood kernel, from its staged voltage) */
     uint64_t launches;       /* kernels launched by the call */
 } fbp_chunk_stats;
 

@@ -45,7 +45,7 @@ class FbpChunkStats(ctypes.Structure):
                 ("ms_lik_tc", ctypes.c_float), ("ms_fixup", ctypes.c_float),
                 ("ms_lik_exact", ctypes.c_float), ("ms_partial_corr", ctypes.c_float),
                 ("ms_screen", ctypes.c_float), ("ms_score", ctypes.c_float),
-                ("ms_overlap_plain", ctypes.c_float), ("pad0", ctypes.c_uint32),
+                ("ms_overlap_plain", ctypes.c_float), ("fixup_runs_queued", ctypes.c_uint32),
                 ("launches", ctypes.c_uint64)]
 
     def as_dict(self):

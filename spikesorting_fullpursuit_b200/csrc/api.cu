@@ -277,6 +277,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         if (hs.error) return fail(FBP_E_DEVICE, "device status error " + std::to_string(hs.error));
         if (overlap) S.flagged += hs.n_flag;
         S.fixups += 4ull * hs.n_fix;   // runs of 4 samples
+        S.fixup_runs_queued += hs.n_fix;
         const uint32_t n = hs.n_spikes;
         if (n == 0) break;
         if ((uint64_t)total + n > capacity) return fail(FBP_E_CAPACITY, "spike capacity exceeded");
@@ -302,6 +303,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     FBP_CUDA(cudaMemcpyAsync(&hs, w.status(), sizeof(hs), cudaMemcpyDeviceToHost, st));
     FBP_CUDA(cudaStreamSynchronize(st));
     S.pair_exact = (plain || !lay.screened) ? hs.pair_items : hs.n_pair_exact;
+    S.fixups += 4ull * hs.n_fix_local;
     S.n_spikes = total;
     S.launches = kclock().launches;
     *n_spikes = total;

@@ -62,7 +62,7 @@ struct DevStatus {
     uint32_t n_conf;        // spikes of this pass overlapping an earlier one
     unsigned long long pair_items;  // items evaluated by the overlap recheck
     uint32_t cand_count;    // candidates appended to the exact-scoring list (per batch)
-    uint32_t pad2;
+    uint32_t n_fix_local;   // runs recomputed inside the likelihood kernel (whole call)
 };
 
 // ---------------------------------------------------------------------------

@@ -42,6 +42,7 @@ namespace {
 constexpr int kTile = 128;         // samples per UMMA tile (M)
 constexpr int kThreads = 192;
 constexpr uint32_t kSpin = 1u << 24;
+constexpr uint32_t kFixCap = 1024;   // runs recomputed in the CTA itself; more go to the global queue
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -185,6 +186,8 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
     float* snorm = reinterpret_cast<float*>(t_rows + P.ntiles);   // [ntiles][C]
     float* bnd = snorm + P.ntiles * d.C;                          // [ntiles][M]
     float* sbias = bnd + P.ntiles * d.M;                          // [M]
+    uint32_t* fq = reinterpret_cast<uint32_t*>(sbias + d.M);      // [kFixCap] runs: t | tile | row | mask
+    uint32_t* nfq = fq + kFixCap;
 
     const uint32_t ksteps = d.W * (P.Cq / 2);
     const uint32_t ngroups = (ksteps + P.group - 1) / P.group;
@@ -196,6 +199,7 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
             mbar_init(&b_empty[s], 1);
         }
         *err = 0;
+        *nfq = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (threadIdx.x < P.ntiles) {
@@ -320,15 +324,27 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
                         uint32_t nz = 0;   // bit k: nibble k non-empty
 #pragma unroll
                         for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
+                        // first into this CTA's own list (recomputed below from the staged
+                        // strips), then the global queue, then inline
                         uint32_t base = 0;
-                        if (lane == 0) base = atomicAdd(&P.status->n_fix, (uint32_t)__popc(nz));
+                        if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
                         base = __shfl_sync(0xffffffffu, base, 0);
                         const uint32_t k = lane >> 2;
                         const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
-                        const bool queued = ((nz >> k) & 1u) && slot < P.fix_cap;
-                        if ((lane & 3u) == 0 && queued)
-                            P.fix[slot] = ((unsigned long long)t << 40) |
-                                          ((unsigned long long)((m >> (4 * k)) & 0xFu) << 32) | s;
+                        const uint32_t nib = (m >> (4 * k)) & 0xFu;
+                        const bool local = nib && slot < kFixCap;
+                        if ((lane & 3u) == 0 && local) fq[slot] = (t << 13) | (i << 11) | (row << 4) | nib;
+                        bool queued = local;
+                        if (nib && !local) {
+                            uint32_t g = 0;
+                            if ((lane & 3u) == 0) {
+                                g = atomicAdd(&P.status->n_fix, 1u);
+                                if (g < P.fix_cap)
+                                    P.fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | s;
+                            }
+                            g = __shfl_sync(0xffffffffu, g, lane & ~3u);
+                            queued = g < P.fix_cap;
+                        }
                         float out = live ? est : 0.f;
                         if (need && !queued) out = exact_likelihood(d, P.V, P.T, b, t, s);
                         if (valid) P.L[(uint64_t)t * d.N + s] = out;
@@ -346,6 +362,48 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
         __syncwarp();
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
+    }
+    // exact recomputation of this CTA's queued runs, all warps, voltage from the
+    // staged strips (row y of channel c of tile i at ((c/4) R8 + y) 16 + (c%4) 4)
+    const uint32_t nq = min(*nfq, kFixCap);
+    if (threadIdx.x == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
+    const uint32_t W = d.W, W4 = W & ~3u, Wp = (W + 3) & ~3u;
+    for (uint32_t qi = threadIdx.x; qi < nq; qi += blockDim.x) {
+        const uint32_t e = fq[qi];
+        const uint32_t t = e >> 13, i = (e >> 11) & 3u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
+        const float* strip = reinterpret_cast<const float*>(A + i * tile_bytes);
+        float a0 = sbias[t], a1 = a0, a2 = a0, a3 = a0;
+        for (uint32_t c = 0; c < d.C; ++c) {
+            const float* vr = strip + ((c >> 2) * P.R8 + r0) * 4 + (c & 3u);   // rows step by 4 floats
+            const float* tr = P.Tp + ((uint64_t)t * d.C + c) * Wp;
+            float w0 = vr[0], w1 = vr[4], w2 = vr[8];
+            uint32_t j = 0;
+            for (; j < W4; j += 4) {
+                const float4 t4 = __ldg(reinterpret_cast<const float4*>(tr + j));
+                const float w3 = vr[4 * (j + 3)], w4 = vr[4 * (j + 4)], w5 = vr[4 * (j + 5)], w6 = vr[4 * (j + 6)];
+                a0 = __fadd_rn(a0, __fmul_rn(t4.x, w0)); a1 = __fadd_rn(a1, __fmul_rn(t4.x, w1));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.x, w2)); a3 = __fadd_rn(a3, __fmul_rn(t4.x, w3));
+                a0 = __fadd_rn(a0, __fmul_rn(t4.y, w1)); a1 = __fadd_rn(a1, __fmul_rn(t4.y, w2));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.y, w3)); a3 = __fadd_rn(a3, __fmul_rn(t4.y, w4));
+                a0 = __fadd_rn(a0, __fmul_rn(t4.z, w2)); a1 = __fadd_rn(a1, __fmul_rn(t4.z, w3));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.z, w4)); a3 = __fadd_rn(a3, __fmul_rn(t4.z, w5));
+                a0 = __fadd_rn(a0, __fmul_rn(t4.w, w3)); a1 = __fadd_rn(a1, __fmul_rn(t4.w, w4));
+                a2 = __fadd_rn(a2, __fmul_rn(t4.w, w5)); a3 = __fadd_rn(a3, __fmul_rn(t4.w, w6));
+                w0 = w4; w1 = w5; w2 = w6;
+            }
+            for (; j < W; ++j) {
+                const float tv = __ldg(tr + j);
+                const float w3 = vr[4 * (j + 3)];
+                a0 = __fadd_rn(a0, __fmul_rn(tv, w0)); a1 = __fadd_rn(a1, __fmul_rn(tv, w1));
+                a2 = __fadd_rn(a2, __fmul_rn(tv, w2)); a3 = __fadd_rn(a3, __fmul_rn(tv, w3));
+                w0 = w1; w1 = w2; w2 = w3;
+            }
+        }
+        float* Lr = P.L + (uint64_t)t * d.N + t_s0[i] + r0;
+        if (mask & 1u) Lr[0] = a0;
+        if (mask & 2u) Lr[1] = a1;
+        if (mask & 4u) Lr[2] = a2;
+        if (mask & 8u) Lr[3] = a3;
     }
 }
 
@@ -497,7 +555,7 @@ bool tc_config(const Dims& d, TcConfig* c)
         c->stages = 3;
         while (c->group > 1 && strips + c->stages * c->group * (size_t)c->Np * 32 > 160 * 1024) c->group >>= 1;
         c->smem = strips + c->stages * (size_t)c->group * c->Np * 32 + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
-                  (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + 1024;
+                  (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + (size_t)kFixCap * 4 + 4 + 1024;
         if (c->smem <= 200 * 1024) return true;
         if (c->ntiles == 1) return false;
         --c->ntiles;
