@@ -129,6 +129,7 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
             if (gb > L->nw) gb = L->nw;
             L->gbatch = gb;
             L->off_g = take(gb * per);
+            L->off_order = take(gb * 4);                // screening order of a batch (by best label)
             L->off_perm = take(M * 4 + 8 + M * 8);      // order, then (8-aligned) non-zero channel masks
             L->off_mx = take(M * M * 4 + 2 * M * 4);   // max -X_ft per pair; max sqrt(E), max E per template
             L->cand_cap = 16ull << 20;                  // exact-scoring candidates per batch

@@ -80,7 +80,7 @@ struct Layout {
     // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
     // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
     // template processing order perm[M]
-    size_t off_et, off_xt, off_xtt, off_g, off_perm, off_mx, off_cand, off_bscr;
+    size_t off_et, off_xt, off_xtt, off_g, off_order, off_perm, off_mx, off_cand, off_bscr;
     uint64_t cand_cap;
     uint64_t gbatch;
     bool screened;

@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
     const uint32_t* __restrict__ flag, DevStatus* status, const uint32_t* __restrict__ best_lab,
     const uint32_t* __restrict__ best_idx, const float* __restrict__ best_lik, unsigned long long* keys,
     const float* __restrict__ mx, unsigned long long* gcand, uint32_t gcand_cap,
-    const unsigned long long* __restrict__ chmask, float* bscratch)
+    const unsigned long long* __restrict__ chmask, float* bscratch, const uint32_t* __restrict__ order)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ ScreenShared sh;
@@ -453,9 +453,10 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
     const float K = 1.01f * 1.05f * u * 2.0f * ((float)d.C * W + d.C + W + 24);
     const uint32_t nflag = status->n_flag;
     unsigned long long exact_n = 0, item_n = 0;
-    for (uint32_t kk = blockIdx.x; kk < kcount; kk += gridDim.x) {
+    for (uint32_t jo = blockIdx.x; jo < kcount; jo += gridDim.x) {
+        const uint32_t kk = order[jo];
         const uint32_t k = k0 + kk;
-        if (k >= nflag) break;
+        if (k >= nflag) continue;
         const uint32_t id = flag[k];
         const uint32_t f = best_lab[id], p = best_idx[id];
         if (window_skipped(d, L, theta, f, p)) continue;
@@ -784,6 +785,34 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
     if (item_n) atomicAdd(&status->pair_items, item_n);
 }
 
+// Screening order of a batch of flagged windows: grouped by best label f (a
+// counting sort), so CTAs running at the same time read the same template's
+// cross-term slices from L2.  Windows past the flagged count go last.
+__global__ void __launch_bounds__(1024) label_order_kernel(Dims d, const uint32_t* __restrict__ flag,
+                                                           const DevStatus* status,
+                                                           const uint32_t* __restrict__ best_lab, uint32_t k0,
+                                                           uint32_t kc, uint32_t* order)
+{
+    extern __shared__ uint32_t hist[];   // [M + 1]
+    const uint32_t nflag = status->n_flag, M = d.M;
+    for (uint32_t i = threadIdx.x; i <= M; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < kc; j += blockDim.x) {
+        const uint32_t f = k0 + j < nflag ? min(best_lab[flag[k0 + j]], M) : M;
+        atomicAdd(&hist[f], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t i = 0; i <= M; ++i) { const uint32_t c = hist[i]; hist[i] = run; run += c; }
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < kc; j += blockDim.x) {
+        const uint32_t f = k0 + j < nflag ? min(best_lab[flag[k0 + j]], M) : M;
+        order[atomicAdd(&hist[f], 1u)] = j;
+    }
+}
+
 // Exact scores of the listed candidates, one thread each: entry = window slot
 // kk (32 bits) | t (12) | a (10) | b (10).  Folds the canonical winner key into
 // keys[k0 + kk].
@@ -935,6 +964,9 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
 #undef FBP_PC
         }
         const uint32_t gb = kc < kScreenGrid ? kc : kScreenGrid;
+        uint32_t* order = w.at<uint32_t>(L.off_order);
+        count_launch();
+        label_order_kernel<<<1, 1024, (d.M + 1) * 4, st>>>(d, w.flag(), w.status(), w.best_lab(), k0, kc, order);
         FBP_CUDA(cudaMemsetAsync(&w.status()->cand_count, 0, 4, st));
         unsigned long long* gcand = w.at<unsigned long long>(L.off_cand);
         {
@@ -942,7 +974,7 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
         screen_kernel<<<gb, kScrThreads, smem_b, st>>>(d, V, T, w.L(), theta, Et, XT, w.at<float>(L.off_xtt), G, k0, kc,
                                                        w.flag(), w.status(), w.best_lab(), w.best_idx(), w.best_lik(),
                                                        w.keys(), w.at<float>(L.off_mx), gcand, (uint32_t)L.cand_cap, chm,
-                                                       bstaged ? nullptr : w.at<float>(L.off_bscr));
+                                                       bstaged ? nullptr : w.at<float>(L.off_bscr), order);
         }
         KScope ks(&fbp_chunk_stats::ms_score, st);
         score_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, w.flag(), k0, w.best_lab(), w.best_idx(), gcand,
