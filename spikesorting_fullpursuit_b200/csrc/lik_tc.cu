@@ -542,16 +542,19 @@ bool tc_config(const Dims& d, TcConfig* c)
     c->Np = (d.M + 15) / 16 * 16;
     if (c->Np > 256) return false;
     c->R8 = (kTile + d.W - 1 + 7) / 8 * 8;
+    // two tiles per CTA: four CTAs fit an SM (TMEM <= 128 columns and about 54 KB of
+    // shared memory each), so one CTA's epilogue and exact recomputations overlap
+    // the others' MMAs (measured faster than four tiles in two CTAs, or one tile)
     c->ntiles = 512 / c->Np;
-    if (c->ntiles > 4) c->ntiles = 4;
+    if (c->ntiles > 2) c->ntiles = 2;
     if (c->ntiles == 0) return false;
     for (;;) {
         const uint32_t cols = c->ntiles * c->Np;
         c->ncols = 32;
         while (c->ncols < cols) c->ncols <<= 1;
         const size_t strips = (size_t)c->ntiles * c->Cq * c->R8 * 16;
-        // template stages of about 12 KB (whole k-steps), three in the ring
-        c->group = (uint32_t)std::max<size_t>(1, (12 * 1024) / ((size_t)c->Np * 32));
+        // template stages of about 6 KB (whole k-steps), three in the ring
+        c->group = (uint32_t)std::max<size_t>(1, (6 * 1024) / ((size_t)c->Np * 32));
         c->stages = 3;
         while (c->group > 1 && strips + c->stages * c->group * (size_t)c->Np * 32 > 160 * 1024) c->group >>= 1;
         c->smem = strips + c->stages * (size_t)c->group * c->Np * 32 + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
