@@ -893,20 +893,28 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     FBP_CUDA(cudaStreamSynchronize(st));
     PcConfig& pc = pc_config();
     pc.Q = 0;
+    // group size: least estimated work, sum over groups of Q x (union channels),
+    // weighted by the measured cost per multiply-add of each group size (two
+    // strip loads feed Q templates; below 4 the shared-memory loads dominate)
+    double best = 0.0;
     for (int Q = 8; Q >= 1; Q >>= 1) {
+        const double eff = Q >= 4 ? 1.0 : (Q == 2 ? 1.2 : 1.6);
         uint32_t cu_max = 0;
+        double work = 0.0;
         for (uint32_t g0 = 0; g0 < d.M; g0 += Q) {
             unsigned long long m = 0ull;
             for (uint32_t q = 0; q < (uint32_t)Q && g0 + q < d.M; ++q) m |= mask[perm[g0 + q]];
             uint32_t cu = 0;
             for (uint32_t c = 0; c < d.C; ++c) cu += (c >= 64 || ((m >> c) & 1ull)) ? 1u : 0u;
             cu_max = cu > cu_max ? cu : cu_max;
+            work += (double)Q * cu;
         }
         const size_t smem = pc_smem_bytes(d, cu_max, Q);
-        if (smem <= 110 * 1024 || (Q == 1 && smem <= 200 * 1024)) {
+        if (!(smem <= 110 * 1024 || (Q == 1 && smem <= 200 * 1024))) continue;
+        if (pc.Q == 0 || work * eff < best) {
             pc.Q = Q;
             pc.smem = smem;
-            break;
+            best = work * eff;
         }
     }
     return FBP_OK;
