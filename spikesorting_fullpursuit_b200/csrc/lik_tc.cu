@@ -163,7 +163,7 @@ __device__ float exact_likelihood(const Dims& d, const float* __restrict__ V, co
     return acc;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
+__global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     const Dims& d = P.d;
@@ -363,24 +363,59 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
     }
-    // exact recomputation of this CTA's queued runs, all warps, voltage from the
-    // staged strips (row y of channel c of tile i at ((c/4) R8 + y) 16 + (c%4) 4)
+    // exact recomputation of this CTA's queued runs, all warps.  The strips are
+    // transposed in place to channel-major rows (channel c of tile i at
+    // (i Cp + c) R8 floats), so a run reads its voltage with aligned 16-byte
+    // loads: 8 consecutive samples per 4 taps, rows of one epilogue warp's band
+    // landing in distinct banks.
     const uint32_t nq = min(*nfq, kFixCap);
     if (threadIdx.x == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
+    if (nq == 0) return;
+    // the strips were written by bulk copies and read by the MMAs (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const uint32_t Cp = P.Cq * 4;
+    {
+        // each 4-channel block of R8 16-byte rows becomes 4 channel rows of R8
+        // floats in the same bytes: one block at a time, read fully, then written
+        constexpr uint32_t kPer = 2;   // R8 <= 256 rows <= kPer * blockDim
+        const float4* src = reinterpret_cast<const float4*>(A);
+        float* dst = reinterpret_cast<float*>(A);
+        for (uint32_t tq = 0; tq < P.ntiles * P.Cq; ++tq) {
+            float4 v[kPer];
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) {
+                const uint32_t row = k * blockDim.x + threadIdx.x;
+                v[k] = row < P.R8 ? src[(size_t)tq * P.R8 + row] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            __syncthreads();
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) {
+                const uint32_t row = k * blockDim.x + threadIdx.x;
+                if (row >= P.R8) continue;
+                float* o = dst + (size_t)4 * tq * P.R8 + row;
+                o[0] = v[k].x;
+                o[P.R8] = v[k].y;
+                o[2 * P.R8] = v[k].z;
+                o[3 * P.R8] = v[k].w;
+            }
+            __syncthreads();
+        }
+    }
     const uint32_t W = d.W, W4 = W & ~3u, Wp = (W + 3) & ~3u;
+    const float* Vt = reinterpret_cast<const float*>(A);
     for (uint32_t qi = threadIdx.x; qi < nq; qi += blockDim.x) {
         const uint32_t e = fq[qi];
         const uint32_t t = e >> 13, i = (e >> 11) & 3u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
-        const float* strip = reinterpret_cast<const float*>(A + i * tile_bytes);
         float a0 = sbias[t], a1 = a0, a2 = a0, a3 = a0;
         for (uint32_t c = 0; c < d.C; ++c) {
-            const float* vr = strip + ((c >> 2) * P.R8 + r0) * 4 + (c & 3u);   // rows step by 4 floats
+            const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0;   // 16-byte aligned
             const float* tr = P.Tp + ((uint64_t)t * d.C + c) * Wp;
-            float w0 = vr[0], w1 = vr[4], w2 = vr[8];
             uint32_t j = 0;
             for (; j < W4; j += 4) {
                 const float4 t4 = __ldg(reinterpret_cast<const float4*>(tr + j));
-                const float w3 = vr[4 * (j + 3)], w4 = vr[4 * (j + 4)], w5 = vr[4 * (j + 5)], w6 = vr[4 * (j + 6)];
+                const float4 lo = *reinterpret_cast<const float4*>(vr + j);
+                const float4 hi = *reinterpret_cast<const float4*>(vr + j + 4);
+                const float w0 = lo.x, w1 = lo.y, w2 = lo.z, w3 = lo.w, w4 = hi.x, w5 = hi.y, w6 = hi.z;
                 a0 = __fadd_rn(a0, __fmul_rn(t4.x, w0)); a1 = __fadd_rn(a1, __fmul_rn(t4.x, w1));
                 a2 = __fadd_rn(a2, __fmul_rn(t4.x, w2)); a3 = __fadd_rn(a3, __fmul_rn(t4.x, w3));
                 a0 = __fadd_rn(a0, __fmul_rn(t4.y, w1)); a1 = __fadd_rn(a1, __fmul_rn(t4.y, w2));
@@ -389,14 +424,11 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_kernel(TcParams P)
                 a2 = __fadd_rn(a2, __fmul_rn(t4.z, w4)); a3 = __fadd_rn(a3, __fmul_rn(t4.z, w5));
                 a0 = __fadd_rn(a0, __fmul_rn(t4.w, w3)); a1 = __fadd_rn(a1, __fmul_rn(t4.w, w4));
                 a2 = __fadd_rn(a2, __fmul_rn(t4.w, w5)); a3 = __fadd_rn(a3, __fmul_rn(t4.w, w6));
-                w0 = w4; w1 = w5; w2 = w6;
             }
-            for (; j < W; ++j) {
+            for (; j < W; ++j) {   // taps past the last multiple of 4
                 const float tv = __ldg(tr + j);
-                const float w3 = vr[4 * (j + 3)];
-                a0 = __fadd_rn(a0, __fmul_rn(tv, w0)); a1 = __fadd_rn(a1, __fmul_rn(tv, w1));
-                a2 = __fadd_rn(a2, __fmul_rn(tv, w2)); a3 = __fadd_rn(a3, __fmul_rn(tv, w3));
-                w0 = w1; w1 = w2; w2 = w3;
+                a0 = __fadd_rn(a0, __fmul_rn(tv, vr[j])); a1 = __fadd_rn(a1, __fmul_rn(tv, vr[j + 1]));
+                a2 = __fadd_rn(a2, __fmul_rn(tv, vr[j + 2])); a3 = __fadd_rn(a3, __fmul_rn(tv, vr[j + 3]));
             }
         }
         float* Lr = P.L + (uint64_t)t * d.N + t_s0[i] + r0;
