@@ -44,6 +44,16 @@ sys.path.insert(0, HERE)
 METRIC = "binary-pursuit Msample·ch/s, chosen vs plain FP32 on B200, ≥99.9% spike match"
 
 
+# DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch of the 60 s slice of the linear16 workload, divided by the windows it processed)
+DRAM_PER_UNIT = {
+    "lik_tc_kernel": (17.1e3, "listed", "profiles/lik_tc_kernel_linear16_60s.md: 106.8 MB / 6,240 windows"),
+    "partial_corr_kernel": (35.8e3, "flagged", "profiles/partial_corr_kernel_linear16_60s.md: 107.3 MB / 3,001 windows"),
+    "screen_kernel": (39.1e3, "flagged", "profiles/screen_kernel_linear16_60s.md: 117.3 MB / 3,001 windows"),
+    "argmax_kernel": (25.8e3, "listed", "profiles/argmax_kernel_linear16_60s.md: 160.8 MB / 6,240 windows"),
+}
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -306,7 +316,15 @@ def main():
                              "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops}
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
     roof = dict(kernels[dom])
-    roof.update({"kernel": dom, "traffic": None, "peak_kind": peak_kind,
+    # DRAM bytes (read + write) per launch: ncu's per-unit figure from the captures in
+    # profiles/ (60 s slice of this workload) times the units of an average launch here
+    per_unit = DRAM_PER_UNIT.get(dom)
+    traffic = None
+    if per_unit is not None:
+        units = {"listed": listed, "flagged": flagged}[per_unit[1]]
+        traffic = {"bytes_per_launch": per_unit[0] * units / max(1, st_stage["passes"]),
+                   "per_unit": per_unit[0], "unit": per_unit[1] + " window", "source": per_unit[2]}
+    roof.update({"kernel": dom, "traffic": traffic, "peak_kind": peak_kind,
                  "note": "peak = measured dense bf16 (TF32 nominal is half of it); hbm = measured copy"})
     launches = int(st_fast["launches"]) * args.steps
 
