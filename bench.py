@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-s", type=float, default=2.0)
+    p.add_argument("--adjoint", action="store_true",
+                   help="time the residual-energy gradient (template refinement) on the 16-ch, 2 min, "
+                        "40-template workload instead of the pursuit")
     p.add_argument("--only-device", action="store_true",
                    help="time the device-resident steps only (no e2e, plain, stage or CPU legs); for profiling")
     return p.parse_args()
@@ -172,6 +175,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.adjoint:
+        run_adjoint(args)
         return
     import torch
     import torch.distributed as dist
@@ -359,6 +365,59 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_adjoint(args):
+    """Residual energy + hand-written adjoint at fixed assignments (template refinement):
+    16-ch linear probe, 2 min at 40 kHz, 40 templates; assignments from one pursuit of the
+    recording, amplitudes ~ N(1, 0.1), shifts ~ U(-0.5, 0.5) samples.  A step is one
+    forward (energy) and one backward (gradients w.r.t. templates, amplitudes, shifts)."""
+    import torch
+    from spikesorting_fullpursuit_b200 import binary_pursuit, synth
+    from spikesorting_fullpursuit_b200.adjoint import residual_energy
+
+    dur = 120.0 if args.duration is None else args.duration
+    V, si, sm, _ = synth.config_recording("linear16", seed=3, duration_s=dur)
+    C, N = V.shape
+    W = si["n_samples_per_chan"]
+    M = sm["templates"].shape[0]
+    si = dict(si, get_adjusted_clips=False)
+    ev, lab, _, _ = binary_pursuit(V, np.float32, si, copy.deepcopy(sm), n_max_shift_inds=W - 1, verbose=False)
+    pre = -int(round(-1.0e-3 * si["sampling_rate"]))
+    idx = np.asarray(ev, dtype=np.int64) - pre
+    rng = np.random.default_rng(3)
+    n = len(idx)
+    dev = torch.device("cuda", 0)
+    Vd = torch.from_numpy(V).to(dev)
+    Td = torch.from_numpy(np.float32(sm["templates"]).reshape(M, C, W)).to(dev).requires_grad_(True)
+    ad = torch.from_numpy(rng.normal(1.0, 0.1, n).astype(np.float32)).to(dev).requires_grad_(True)
+    sd = torch.from_numpy(rng.uniform(-0.5, 0.5, n).astype(np.float32)).to(dev).requires_grad_(True)
+    idd = torch.from_numpy(idx).to(dev)
+    ld = torch.from_numpy(np.asarray(lab, dtype=np.int64)).to(dev)
+
+    def step():
+        Td.grad = ad.grad = sd.grad = None
+        e = residual_energy(Vd, Td, idd, ld, ad, sd)
+        e.backward()
+        return e
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        step()
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / args.steps
+    print(json.dumps({
+        "metric": "residual-energy gradient (templates, amplitudes, shifts) Msample*ch/s", "value": C * N / (ms * 1e-3) / 1e6,
+        "unit": "Msample*ch/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "f64 sums of f32 inputs", "data": "synthetic",
+        "config": {"workload": "adjoint: %d ch x %d samples (%.0f s at %d Hz), %d templates x %d samples, %d spikes "
+                               "(from one pursuit), linear-interpolation shifts" % (C, N, N / si["sampling_rate"],
+                                                                                   si["sampling_rate"], M, W, n)}}))
 
 
 def cpu_baseline(args):

@@ -161,6 +161,28 @@ int fbp_residual_noalloc(const fbp_dims* dims, float* voltage, const float* temp
                          const uint32_t* spike_idx, const uint32_t* spike_lab, uint32_t n,
                          void* stream);
 
+/* Residual energy of a fixed spike assignment, for template refinement (no
+ * counterpart in the reference):
+ *   E = sum_{c,x} (v[c][x] - sum_k a_k T~_k[c][x - s_k])^2
+ * with spike k at onset s_k = spike_idx[k] (ascending), template spike_lab[k],
+ * amplitude a_k = amplitude[k] and fractional shift tau_k = shift[k] in (-1, 1)
+ * samples: T~(c, j) = (1-|tau|) T[c][j] + |tau| T[c][j + dir], dir = -1 for
+ * tau >= 0 and +1 for tau < 0, j in [-1, W], T = 0 outside [0, W); samples
+ * outside [0, N) are not modelled.  Computed in FP64 from float32 inputs; *loss
+ * is device memory. */
+int fbp_adjoint_loss(const fbp_dims* dims, const float* voltage, const float* templates,
+                     const uint32_t* spike_idx, const uint32_t* spike_lab, const float* amplitude,
+                     const float* shift, uint32_t n_spikes, double* loss, void* stream);
+
+/* scale * dE/d(templates, amplitude, shift) for fbp_adjoint_loss's E.  Residual
+ * tiles are recomputed per spike (nothing kept from the loss call); sums in
+ * FP64.  grad_templates64 is FP64 scratch [M][C][W] (overwritten),
+ * grad_templates float32 [M][C][W], grad_amplitude and grad_shift float32 [n]. */
+int fbp_adjoint_grad(const fbp_dims* dims, const float* voltage, const float* templates,
+                     const uint32_t* spike_idx, const uint32_t* spike_lab, const float* amplitude,
+                     const float* shift, uint32_t n_spikes, double scale, double* grad_templates64,
+                     float* grad_templates, float* grad_amplitude, float* grad_shift, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

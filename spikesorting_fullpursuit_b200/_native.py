@@ -25,7 +25,8 @@ FBP_TIMING = 0x4
 
 # every function include/fbp.h declares
 EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_pursue_chunk",
-           "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc")
+           "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc",
+           "fbp_adjoint_loss", "fbp_adjoint_grad")
 NOALLOC_MAX_SPIKES = 65536
 
 
@@ -85,6 +86,10 @@ def lib():
     L.fbp_residual.restype = ctypes.c_int
     L.fbp_residual_noalloc.argtypes = [P(FbpDims), vp, vp, vp, vp, u32, vp]
     L.fbp_residual_noalloc.restype = ctypes.c_int
+    L.fbp_adjoint_loss.argtypes = [P(FbpDims), vp, vp, vp, vp, vp, vp, u32, vp, vp]
+    L.fbp_adjoint_loss.restype = ctypes.c_int
+    L.fbp_adjoint_grad.argtypes = [P(FbpDims), vp, vp, vp, vp, vp, vp, u32, ctypes.c_double, vp, vp, vp, vp, vp]
+    L.fbp_adjoint_grad.restype = ctypes.c_int
     _lib = L
     return L
 
