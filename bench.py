@@ -64,7 +64,7 @@ def parse():
     p.add_argument("--duration", type=float, default=None, help="seconds of recording (default: config's)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--cpu-sample-s", type=float, default=2.0)
+    p.add_argument("--cpu-sample-s", type=float, default=1.0)
     p.add_argument("--adjoint", action="store_true",
                    help="time the residual-energy gradient (template refinement) on the 16-ch, 2 min, "
                         "40-template workload instead of the pursuit")
@@ -140,16 +140,25 @@ def run_reference(args, rank):
     sys.path.insert(0, os.path.join(HERE, "oracle"))
     from spikesorting_fullpursuit_b200 import synth
     import ref_host
+    # warm-up steps load the library and touch the code path on a short slice; the timed
+    # slice is sized from the warm-up rate so that the K timed steps take about 150 s
+    Vw, siw, smw, _ = synth.config_recording(args.config, seed=1, duration_s=0.1)
+    Ww = siw["n_samples_per_chan"]
+    rate = None
+    for _ in range(args.warmup):
+        t0 = time.perf_counter()
+        ref_host.binary_pursuit(Vw, siw, copy.deepcopy(smw), n_max_shift_inds=Ww - 1)
+        rate = Vw.shape[1] / (time.perf_counter() - t0)   # samples per second
     sample_s = args.cpu_sample_s
+    if rate:
+        sample_s = float(np.clip(150.0 / max(1, args.steps) * rate / siw["sampling_rate"], 0.25, args.cpu_sample_s))
     V, si, sm, _ = synth.config_recording(args.config, seed=1, duration_s=sample_s)
     W = si["n_samples_per_chan"]
     times = []
-    for i in range(args.warmup + args.steps):
+    for _ in range(args.steps):
         t0 = time.perf_counter()
         ref_host.binary_pursuit(V, si, copy.deepcopy(sm), n_max_shift_inds=W - 1)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            times.append(dt)
+        times.append(time.perf_counter() - t0)
     tot = float(np.sum(times))
     value = V.shape[0] * V.shape[1] * len(times) / tot / 1e6
     cores = ref_host.threads()
