@@ -100,3 +100,28 @@ def test_product_does_not_import_oracle():
             if f.endswith(".py"):
                 src = open(os.path.join(root, f)).read()
                 assert "oracle" not in re.findall(r"^\s*(?:import|from)\s+(\w+)", src, re.M), f
+
+
+def test_adjoint_arguments_fail_before_any_device_call(lib):
+    P = ctypes.c_void_p
+    fake = P(16)   # never dereferenced: validation rejects the call first
+    d = _native.dims(4, 1000, 3, 21, 0)
+    loss = ctypes.c_void_p(32)
+    # null dims, zero sizes, null inputs, null spike arrays with spikes, null outputs
+    assert lib.fbp_adjoint_loss(None, fake, fake, fake, fake, fake, fake, 1, loss, None) == _native.FBP_E_ARG
+    for bad in (_native.dims(0, 1000, 3, 21, 0), _native.dims(4, 0, 3, 21, 0), _native.dims(4, 1000, 0, 21, 0),
+                _native.dims(4, 1000, 3, 0, 0)):
+        assert lib.fbp_adjoint_loss(ctypes.byref(bad), fake, fake, fake, fake, fake, fake, 1, loss,
+                                    None) == _native.FBP_E_ARG
+    assert lib.fbp_adjoint_loss(ctypes.byref(d), None, fake, fake, fake, fake, fake, 1, loss, None) == _native.FBP_E_ARG
+    assert lib.fbp_adjoint_loss(ctypes.byref(d), fake, fake, None, fake, fake, fake, 1, loss, None) == _native.FBP_E_ARG
+    assert lib.fbp_adjoint_loss(ctypes.byref(d), fake, fake, fake, fake, fake, fake, 1, None, None) == _native.FBP_E_ARG
+    assert lib.fbp_adjoint_grad(ctypes.byref(d), fake, fake, fake, fake, fake, fake, 1, ctypes.c_double(1.0),
+                                None, fake, fake, fake, None) == _native.FBP_E_ARG
+    assert lib.fbp_adjoint_grad(ctypes.byref(d), fake, fake, fake, fake, fake, fake, 1, ctypes.c_double(1.0),
+                                fake, fake, None, fake, None) == _native.FBP_E_ARG
+    # one spike's FP64 residual tile (C x (W + 2) doubles) must fit in shared memory
+    big = _native.dims(256, 100000, 3, 101, 0)
+    assert lib.fbp_adjoint_loss(ctypes.byref(big), fake, fake, fake, fake, fake, fake, 1, loss,
+                                None) == _native.FBP_E_ARG
+    assert b"tile" in lib.fbp_last_error()
