@@ -572,7 +572,9 @@ bool tc_config(const Dims& d, TcConfig* c)
     const uint32_t Cp = (d.C + 7) / 8 * 8;
     c->Cq = Cp / 4;
     c->Np = (d.M + 15) / 16 * 16;
-    if (c->Np > 256) return false;
+    // up to 128 template columns (two tiles take at most 256 TMEM columns, so two or
+    // more CTAs share an SM); larger template sets use the exact FP32 likelihood kernel
+    if (c->Np > 128) return false;
     c->R8 = (kTile + d.W - 1 + 7) / 8 * 8;
     // two tiles per CTA: four CTAs fit an SM (TMEM <= 128 columns and about 54 KB of
     // shared memory each), so one CTA's epilogue and exact recomputations overlap
