@@ -293,7 +293,12 @@ def main():
     n_sp = len(out[0])
 
     plain = None
-    if not args.no_plain:
+    # the plain path's brute-force recheck costs (2S+1)^2 * M * C * W multiply-adds per flagged
+    # window; above ~1e10 (e.g. 64 ch, 200 templates) one pursuit would take hours
+    plain_work = (2 * S + 1) ** 2 * M * C * W
+    if not args.no_plain and plain_work > 1e10:
+        plain = {"skipped": "brute-force recheck of %.1e multiply-adds per flagged window" % plain_work}
+    elif not args.no_plain:
         ms_plain, st_plain, res_plain = run_mode(_native.FBP_PLAIN_FP32, 1, 1)
         a = set(zip(res_fast[0].tolist(), res_fast[1].tolist()))
         b = set(zip(res_plain[0].tolist(), res_plain[1].tolist()))
