@@ -32,11 +32,63 @@ def shard_segments(lengths: Sequence[int], world_size: int) -> List[List[int]]:
     return shards
 
 
-def pursue_segments(segments, pursue: Callable = None, group=None, **kwargs):
+def _run_local(segments, mine, lengths, pursue, streams, kwargs):
+    """Results of this rank's segments, by segment index.  With streams > 1 the
+    segments (longest first) are taken by that many worker threads; on a CUDA
+    device each worker issues its segments on a stream of its own, so several
+    segments' kernels run on the GPU at once (every call keeps its own
+    workspace; the library's per-call state is thread-local)."""
+    if streams <= 1 or len(mine) <= 1:
+        return {i: pursue(*segments[i], **kwargs) for i in mine}
+    import queue
+    import threading
+
+    import torch
+
+    use_cuda = torch.cuda.is_available()
+    device = torch.cuda.current_device() if use_cuda else None
+    todo = queue.Queue()
+    for i in sorted(mine, key=lambda k: (-lengths[k], k)):
+        todo.put(i)
+    out, errors = {}, []
+
+    def worker():
+        stream = None
+        if use_cuda:
+            torch.cuda.set_device(device)
+            stream = torch.cuda.Stream(device)
+        while True:   # a failure does not stop the others: the lowest failing index is re-raised
+            try:
+                i = todo.get_nowait()
+            except queue.Empty:
+                return
+            try:
+                if stream is not None:
+                    with torch.cuda.stream(stream):
+                        out[i] = pursue(*segments[i], **kwargs)
+                    stream.synchronize()
+                else:
+                    out[i] = pursue(*segments[i], **kwargs)
+            except BaseException as exc:   # re-raised in the caller, in segment order
+                errors.append((i, exc))
+
+    threads = [threading.Thread(target=worker) for _ in range(min(streams, len(mine)))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise min(errors, key=lambda e: e[0])[1]
+    return out
+
+
+def pursue_segments(segments, pursue: Callable = None, group=None, streams: int = 1, **kwargs):
     """Run ``pursue(*segment)`` for every segment on the rank that owns it.
 
     segments: sequence of argument tuples for ``pursue`` (by default the
     drop-in binary_pursuit: (voltage, v_dtype, sort_info, separability_metrics)).
+    streams: segments of one rank pursued at once (worker threads, one CUDA
+    stream each); 1 runs them one after another.
     Returns the list of results in segment order on every rank.  Without an
     initialised process group everything runs locally."""
     import torch.distributed as dist
@@ -48,7 +100,7 @@ def pursue_segments(segments, pursue: Callable = None, group=None, **kwargs):
     rank = dist.get_rank(group) if dist_on else 0
     lengths = [int(seg[0].shape[1]) for seg in segments]
     mine = shard_segments(lengths, world)[rank]
-    local = {i: pursue(*segments[i], **kwargs) for i in mine}
+    local = _run_local(segments, mine, lengths, pursue, int(streams), kwargs)
     if not dist_on:
         return [local[i] for i in range(len(segments))]
     gathered = [None] * world

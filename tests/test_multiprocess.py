@@ -68,3 +68,22 @@ def test_two_ranks_gather_every_segment_in_order():
 def test_without_process_group_runs_locally():
     res = pursue_segments(_segments(), pursue=_fake_pursue)
     assert len(res) == 5 and all(r[1][0] == k for k, r in enumerate(res) if r[1].size)
+
+
+def test_concurrent_workers_return_results_in_segment_order():
+    segs = _segments()
+    want = pursue_segments(segs, pursue=_fake_pursue)
+    got = pursue_segments(segs, pursue=_fake_pursue, streams=3)
+    assert len(got) == len(want)
+    for g, w in zip(got, want):
+        assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])
+
+
+def test_concurrent_workers_reraise_the_first_failing_segment():
+    def pursue(voltage, tag):
+        if tag in (1, 3):
+            raise RuntimeError("segment %d" % tag)
+        return _fake_pursue(voltage, tag)
+
+    with pytest.raises(RuntimeError, match="segment 1"):
+        pursue_segments(_segments(), pursue=pursue, streams=4)
