@@ -339,12 +339,13 @@ def main():
     # DRAM bytes (read + write) per launch: ncu's per-unit figure from the captures in
     # profiles/ (60 s slice of this workload) times the units of an average launch here
     per_unit = DRAM_PER_UNIT.get(dom)
-    traffic = None
+    traffic, traffic_detail = None, None
     if per_unit is not None:
         units = {"listed": listed, "flagged": flagged}[per_unit[1]]
-        traffic = {"bytes_per_launch": per_unit[0] * units / max(1, st_stage["passes"]),
-                   "per_unit": per_unit[0], "unit": per_unit[1] + " window", "source": per_unit[2]}
-    roof.update({"kernel": dom, "traffic": traffic, "peak_kind": peak_kind,
+        traffic = per_unit[0] * units / max(1, st_stage["passes"])   # bytes per launch
+        traffic_detail = {"bytes_per_unit": per_unit[0], "unit": per_unit[1] + " window",
+                          "launches_per_step": st_stage["passes"], "source": per_unit[2]}
+    roof.update({"kernel": dom, "traffic": traffic, "traffic_detail": traffic_detail, "peak_kind": peak_kind,
                  "note": "peak = measured dense bf16 (TF32 nominal is half of it); hbm = measured copy"})
     launches = int(st_fast["launches"]) * args.steps
 
