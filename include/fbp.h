@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define FBP_ABI_VERSION 2
+#define FBP_ABI_VERSION 3
 
 typedef enum fbp_status {
     FBP_OK = 0,
@@ -49,6 +49,9 @@ typedef struct fbp_dims {
     uint32_t n_max_shift;  /* S, n_max_shift_inds of the overlap recheck */
     uint32_t work_group;   /* work-group size whose order the results follow (power of two, 256) */
 } fbp_dims;
+
+/* Passes whose spike counts fbp_chunk_stats keeps. */
+#define FBP_PASS_RING 64
 
 /* Counters of one fbp_pursue_chunk call. */
 typedef struct fbp_chunk_stats {
@@ -76,6 +79,9 @@ typedef struct fbp_chunk_stats {
     uint32_t fixup_runs_queued; /* runs recomputed by the separate fixup kernel (the others inside
                                    the likelihood kernel, from its staged voltage) */
     uint64_t launches;       /* kernels launched by the call */
+    /* spikes added by each pass: pass p (1-based) at [(p - 1) % FBP_PASS_RING], so
+       after more than FBP_PASS_RING passes the ring holds the most recent ones */
+    uint32_t pass_spikes[FBP_PASS_RING];
 } fbp_chunk_stats;
 
 /* Option bit: record per-stage and per-kernel device times in the stats
@@ -103,9 +109,16 @@ size_t fbp_workspace_bytes(const fbp_dims* dims, uint32_t flags);
  *   theta     float32[M], neuron_lower_thresholds (binary_pursuit_parallel.py:262)
  *   spike_idx, spike_lab  uint32[capacity]: spike onsets (chunk-relative) and
  *             template rows, pass by pass, each pass in window order
- *   n_spikes  host out: number of spikes written
+ *   n_spikes  host out: number of spikes written; after FBP_E_CAPACITY, a lower
+ *             bound of the capacity the chunk needs (the voltage is then partly
+ *             pursued: restore it before a retry)
  *   stats     host out, may be NULL
- *   max_passes  0 = no limit
+ *   max_passes  0 = no limit; otherwise the call fails with FBP_E_PASSES when pass
+ *             max_passes still adds spikes (stats then hold the counters so far,
+ *             including the spikes of the recent passes).  The reference's own
+ *             loop has no limit (binary_pursuit_parallel.py:907); every pass adds
+ *             at least one spike, so a pursuit of N samples and window W ends
+ *             within ceil(N/W) * (spikes per window) passes.
  * The call synchronises with `stream` once per pass to read the pass's spike
  * count. */
 int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* voltage,

@@ -28,6 +28,8 @@ EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_purs
            "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc",
            "fbp_adjoint_loss", "fbp_adjoint_grad")
 NOALLOC_MAX_SPIKES = 65536
+PASS_RING = 64
+ABI_VERSION = 3
 
 
 class FbpDims(ctypes.Structure):
@@ -47,10 +49,16 @@ class FbpChunkStats(ctypes.Structure):
                 ("ms_lik_exact", ctypes.c_float), ("ms_partial_corr", ctypes.c_float),
                 ("ms_screen", ctypes.c_float), ("ms_score", ctypes.c_float),
                 ("ms_overlap_plain", ctypes.c_float), ("fixup_runs_queued", ctypes.c_uint32),
-                ("launches", ctypes.c_uint64)]
+                ("launches", ctypes.c_uint64), ("pass_spikes", ctypes.c_uint32 * PASS_RING)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        out = {k: getattr(self, k) for k, _ in self._fields_}
+        # spikes per pass, oldest first (the ring keeps the last PASS_RING passes)
+        p = int(self.passes)
+        ring = list(self.pass_spikes)
+        first = max(1, p - PASS_RING + 1)
+        out["pass_spikes"] = [ring[(q - 1) % PASS_RING] for q in range(first, p + 1)]
+        return out
 
 
 class FbpError(RuntimeError):
@@ -70,6 +78,9 @@ def lib():
     if not os.path.exists(LIB_PATH):
         raise OSError("libfbp.so is not built; run spikesorting_fullpursuit_b200/build.py")
     L = ctypes.CDLL(LIB_PATH)
+    L.fbp_abi_version.restype = ctypes.c_int
+    if L.fbp_abi_version() != ABI_VERSION:
+        raise OSError("libfbp.so has ABI %d, this binding needs %d: rebuild it" % (L.fbp_abi_version(), ABI_VERSION))
     P, vp, u32, sz = ctypes.POINTER, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_size_t
     L.fbp_abi_version.restype = ctypes.c_int
     L.fbp_last_error.restype = ctypes.c_char_p

@@ -28,6 +28,12 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() else None
 
 
+def _stream(t):
+    # the kernels run on torch's current stream of the tensor's device, in order
+    # with the work that produced their inputs and the work that reads their outputs
+    return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
 class _ResidualEnergy(torch.autograd.Function):
     @staticmethod
     def forward(ctx, voltage, templates, spike_idx, spike_lab, amplitude, shift):
@@ -45,7 +51,8 @@ class _ResidualEnergy(torch.autograd.Function):
         d = _native.dims(C, N, M, W, 0)
         loss = torch.zeros(1, dtype=torch.float64, device=voltage.device)
         _native.check(_native.lib().fbp_adjoint_loss(ctypes.byref(d), _ptr(V), _ptr(T), _ptr(idx), _ptr(lab),
-                                                     _ptr(amp), _ptr(tau), int(idx.numel()), _ptr(loss), None))
+                                                     _ptr(amp), _ptr(tau), int(idx.numel()), _ptr(loss),
+                                                     _stream(V)))
         ctx.save_for_backward(V, T, idx, lab, amp, tau, order)
         ctx.shape = (C, N, M, W)
         ctx.t_shape, ctx.t_dtype = templates.shape, templates.dtype
@@ -65,7 +72,7 @@ class _ResidualEnergy(torch.autograd.Function):
         scale = float(grad_out.item())
         _native.check(_native.lib().fbp_adjoint_grad(ctypes.byref(d), _ptr(V), _ptr(T), _ptr(idx), _ptr(lab),
                                                      _ptr(amp), _ptr(tau), int(n), ctypes.c_double(scale),
-                                                     _ptr(g64), _ptr(gT), _ptr(ga), _ptr(gs), None))
+                                                     _ptr(g64), _ptr(gT), _ptr(ga), _ptr(gs), _stream(V)))
         inv = torch.empty_like(order)
         inv[order] = torch.arange(n, device=order.device)
         grad_T = gT.reshape(ctx.t_shape).to(ctx.t_dtype) if ctx.needs_input_grad[1] else None

@@ -243,7 +243,13 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     uint32_t nlist = d.nw, total = 0;
     api_detail::StageTimer tm;
     for (int32_t pass = 1;; ++pass) {
-        if (max_passes > 0 && pass > max_passes) return fail(FBP_E_PASSES, "pass limit reached");
+        if (max_passes > 0 && pass > max_passes) {
+            S.n_spikes = total;
+            S.launches = kclock().launches;
+            *n_spikes = total;
+            return fail(FBP_E_PASSES, "pass limit reached: pass " + std::to_string(max_passes) +
+                                          " still added spikes (" + std::to_string(total) + " so far)");
+        }
         S.passes = pass;
         S.listed += nlist;
         FBP_CUDA(cudaMemsetAsync(&w.status()->chain_overflow, 0, 8, st));
@@ -280,8 +286,13 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         S.fixups += 4ull * hs.n_fix;   // runs of 4 samples
         S.fixup_runs_queued += hs.n_fix;
         const uint32_t n = hs.n_spikes;
+        S.pass_spikes[(pass - 1) % FBP_PASS_RING] = n;
         if (n == 0) break;
-        if ((uint64_t)total + n > capacity) return fail(FBP_E_CAPACITY, "spike capacity exceeded");
+        if ((uint64_t)total + n > capacity) {
+            S.n_spikes = total;
+            *n_spikes = total + n;   // at least this many outputs are needed
+            return fail(FBP_E_CAPACITY, "spike capacity exceeded");
+        }
         FBP_CUDA(cudaMemcpyAsync(spike_idx + total, w.pidx(), (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
         FBP_CUDA(cudaMemcpyAsync(spike_lab + total, w.plab(), (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
         FBP_CUDA(cudaMemsetAsync(w.orech(), 0, d.nw, st));

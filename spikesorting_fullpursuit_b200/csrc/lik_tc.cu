@@ -41,7 +41,7 @@ namespace {
 
 constexpr int kTile = 128;         // samples per UMMA tile (M)
 constexpr int kThreads = 192;
-constexpr uint32_t kSpin = 1u << 24;
+constexpr uint64_t kWaitNs = 250ull * 1000ull * 1000ull;   // longest mbarrier wait (global timer)
 constexpr uint32_t kFixCap = 1024;   // runs recomputed in the CTA itself; more go to the global queue
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -73,12 +73,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait: false after kSpin unsuccessful polls.
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: false once the phase has not completed within kWaitNs of
+// device time (the global nanosecond timer), checked every 64 polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {
-    for (uint32_t i = 0; i < kSpin; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > kWaitNs) return false;
+    }
 }
 
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
@@ -576,9 +588,10 @@ bool tc_config(const Dims& d, TcConfig* c)
     // more CTAs share an SM); larger template sets use the exact FP32 likelihood kernel
     if (c->Np > 128) return false;
     c->R8 = (kTile + d.W - 1 + 7) / 8 * 8;
-    // two tiles per CTA: four CTAs fit an SM (TMEM <= 128 columns and about 54 KB of
-    // shared memory each), so one CTA's epilogue and exact recomputations overlap
-    // the others' MMAs (measured faster than four tiles in two CTAs, or one tile)
+    // two tiles per CTA: up to 48 template columns four CTAs fit an SM (TMEM <= 128
+    // columns and about 54 KB of shared memory each), so one CTA's epilogue and exact
+    // recomputations overlap the others' MMAs (measured faster than four tiles in two
+    // CTAs, or one tile); wider template sets fit fewer CTAs (see the TMEM rule below)
     c->ntiles = 512 / c->Np;
     if (c->ntiles > 2) c->ntiles = 2;
     if (c->ntiles == 0) return false;
@@ -593,6 +606,11 @@ bool tc_config(const Dims& d, TcConfig* c)
         while (c->group > 1 && strips + c->stages * c->group * (size_t)c->Np * 32 > 160 * 1024) c->group >>= 1;
         c->smem = strips + c->stages * (size_t)c->group * c->Np * 32 + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
                   (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + (size_t)kFixCap * 4 + 4 + 1024;
+        // CTAs resident on one SM must not ask for more than its 512 TMEM columns
+        // together (a blocked tcgen05.alloc would wait for another CTA to finish):
+        // ask for enough shared memory that at most 512 / ncols of them fit
+        const uint32_t fit = 512 / c->ncols;   // 1..4 (at most 4 by the launch bounds)
+        if (fit < 4) c->smem = std::max<size_t>(c->smem, (228 * 1024) / (fit + 1) + 1024);
         if (c->smem <= 200 * 1024) return true;
         if (c->ntiles == 1) return false;
         --c->ntiles;

@@ -42,12 +42,14 @@ extern "C" int fbp_residual_noalloc(const fbp_dims* dims, float* voltage, const 
                                     void* stream)
 {
     namespace na = fbp::noalloc_detail;
+    set_error("");
     Layout lay;
     if (!make_layout(dims, FBP_PLAIN_FP32, &lay)) return fail(FBP_E_ARG, "invalid dims");
     if (n == 0) return FBP_OK;
     if (n > na::kMaxSpikes)
         return fail(FBP_E_ARG, "fbp_residual_noalloc: n exceeds FBP_NOALLOC_MAX_SPIKES (65536)");
     if (!voltage || !templates || !spike_idx || !spike_lab) return fail(FBP_E_ARG, "null pointer argument");
+    if (n > lay.nw) return fail(FBP_E_ARG, "more spikes than windows in the chunk");
     int dev = 0;
     FBP_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= na::kMaxDevices) return fail(FBP_E_ARG, "device ordinal out of range");

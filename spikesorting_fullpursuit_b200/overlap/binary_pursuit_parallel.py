@@ -14,7 +14,8 @@ the C ABI of include/fbp.h) on PyTorch-owned device buffers.  Chunking follows
 the reference's device-memory planner with this GPU's memory, so chunk
 boundaries (and the duplicate spikes the reference leaves in the 3W chunk
 overlaps) are the reference's.  Results equal the reference kernels run with
-their work-groups in order (see include/fbp.h and DESIGN.md).
+their work-groups in order: where the reference's outcome depends on which
+work-item runs first, the outcome of in-order execution is the one reproduced.
 
 Differences, all documented:
 * ``kernels_path`` is accepted and ignored (there is no OpenCL source).
@@ -22,14 +23,19 @@ Differences, all documented:
   reference raises UnboundLocalError (binary_pursuit_parallel.py:1369-1371
   releases buffers it never created); this implementation returns the empty
   result it was meant to return.
+* The reference's pass loop has no limit (binary_pursuit_parallel.py:907);
+  here a chunk that still adds spikes after ``max_passes`` passes raises
+  FbpError (status FBP_E_PASSES) instead of running on.
 * Keyword-only extras: ``mode`` ("fast": tensor-core likelihood and screened
   overlap recheck, both exact; "plain": scalar FP32 kernels), ``device``,
   ``work_group_size`` (the reference's kernel work-group size, 256, whose
-  execution order the results follow), ``verbose``, ``return_stats``.
+  execution order the results follow), ``max_passes``, ``verbose``,
+  ``return_stats``.
 """
 from __future__ import annotations
 
 import ctypes
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -37,6 +43,8 @@ from .. import _native
 from ..processing.conversions import time_window_to_samples
 
 WORK_GROUP_SIZE = 256
+MAX_PASSES = 2048          # default pass limit of one chunk
+MAX_CAPACITY_RETRIES = 4   # re-runs of a chunk whose spikes outgrew the output buffers
 
 
 def plan_chunks(n_samples, n_chans, n_templates, template_samples_per_chan, sampling_rate,
@@ -79,17 +87,74 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+class _Uploader:
+    """Host -> device copy of voltage chunks through pinned staging slabs.
+
+    Host threads convert and copy pieces of the chunk (one channel row range
+    each) into page-locked slabs while the copy engine moves the previous
+    pieces to the device on a stream of its own; ``upload`` makes the caller's
+    stream wait for the last piece.  The source may be any real dtype and any
+    row-strided view: the float32 conversion happens in the slab copy."""
+
+    SLAB_FLOATS = 4 << 20    # 16 MB per slab
+    N_SLABS = 8
+    N_THREADS = 4
+
+    def __init__(self, torch, dev):
+        self.torch = torch
+        self.dev = dev
+        self.slabs = None
+        self.events = [None] * self.N_SLABS
+        self.stream = torch.cuda.Stream(dev)
+        self.pool = ThreadPoolExecutor(self.N_THREADS)
+
+    def upload(self, host, dst):
+        torch = self.torch
+        if self.slabs is None:
+            self.slabs = [torch.empty(self.SLAB_FLOATS, dtype=torch.float32, pin_memory=True)
+                          for _ in range(self.N_SLABS)]
+        C, N = host.shape
+        step = self.SLAB_FLOATS
+        pieces = [(c, a, min(N, a + step)) for c in range(C) for a in range(0, N, step)]
+        caller = torch.cuda.current_stream(self.dev)
+        self.stream.wait_stream(caller)   # dst may still be read by earlier work
+        half = self.N_SLABS // 2
+        for w0 in range(0, len(pieces), half):
+            wave = pieces[w0:w0 + half]
+            slots = [((w0 // half) % 2) * half + k for k in range(len(wave))]
+            for k in slots:
+                if self.events[k] is not None:
+                    self.events[k].synchronize()
+
+            def fill(job):
+                (c, a, b), k = job
+                np.copyto(self.slabs[k].numpy()[:b - a], host[c, a:b], casting="unsafe")
+
+            list(self.pool.map(fill, zip(wave, slots)))
+            with torch.cuda.stream(self.stream):
+                for (c, a, b), k in zip(wave, slots):
+                    dst[c, a:b].copy_(self.slabs[k][:b - a], non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(self.stream)
+                    self.events[k] = ev
+        caller.wait_stream(self.stream)
+
+    def close(self):
+        self.pool.shutdown(wait=True)
+
+
 class _Pursuer:
     """Device buffers and the C-ABI calls for one binary_pursuit() call."""
 
     def __init__(self, torch, dev, n_chans, templates, bias, theta, W, S, max_chunk, flags,
-                 work_group_size):
+                 work_group_size, max_passes):
         self.torch = torch
         self.dev = dev
         self.C, self.W, self.S = n_chans, W, S
         self.M = templates.shape[0]
         self.flags = flags
         self.wg = work_group_size
+        self.max_passes = int(max_passes)
         self.T = torch.from_numpy(np.ascontiguousarray(templates, dtype=np.float32)).to(dev)
         self.bias = torch.from_numpy(np.ascontiguousarray(bias, dtype=np.float32)).to(dev)
         self.theta = torch.from_numpy(np.ascontiguousarray(theta, dtype=np.float32)).to(dev)
@@ -98,18 +163,24 @@ class _Pursuer:
         if nbytes == 0:
             raise ValueError("invalid binary pursuit sizes for the GPU library")
         self.ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        self.V = torch.empty((n_chans, max_chunk), dtype=torch.float32, device=dev)
+        self.up = _Uploader(torch, dev)
         self.stats = []
 
     def chunk(self, host_chunk, clips):
+        """Pursue one chunk (``host_chunk``: C x N view of the caller's voltage)."""
         torch = self.torch
         C, N = host_chunk.shape
         d = _native.dims(C, N, self.M, self.W, self.S, self.wg)
-        V = torch.from_numpy(host_chunk).to(self.dev)
+        V = self.V[:, :N] if N == self.V.shape[1] else self.V.view(-1)[:C * N].view(C, N)
+        self.up.upload(host_chunk, V)
         nw = (N + self.W - 1) // self.W
-        cap = 4 * nw + 1024
+        # every pass adds at most one spike per window
+        most = nw * self.max_passes if self.max_passes > 0 else 0xFFFFFFFF
+        cap = min(4 * nw + 1024, most, 0xFFFFFFFF)
         stream = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
         L = _native.lib()
-        while True:
+        for attempt in range(MAX_CAPACITY_RETRIES + 1):
             idx = torch.empty(cap, dtype=torch.int32, device=self.dev)
             lab = torch.empty(cap, dtype=torch.int32, device=self.dev)
             n = ctypes.c_uint32(0)
@@ -117,14 +188,16 @@ class _Pursuer:
             rc = L.fbp_pursue_chunk(ctypes.byref(d), self.flags, _ptr(V), _ptr(self.T),
                                     _ptr(self.bias), _ptr(self.theta), _ptr(self.ws),
                                     self.ws.numel(), _ptr(idx), _ptr(lab), cap, ctypes.byref(n),
-                                    ctypes.byref(st), 0, stream)
-            if rc == _native.FBP_E_CAPACITY:
-                cap *= 4
-                V.copy_(torch.from_numpy(host_chunk))
-                continue
-            _native.check(rc)
-            break
+                                    ctypes.byref(st), self.max_passes, stream)
+            if rc != _native.FBP_E_CAPACITY:
+                break
+            if cap >= min(most, 0xFFFFFFFF) or attempt == MAX_CAPACITY_RETRIES:
+                _native.check(rc)
+            # n holds a lower bound of what the chunk needs; the voltage was partly pursued
+            cap = int(min(max(4 * cap, 2 * n.value), most, 0xFFFFFFFF))
+            self.up.upload(host_chunk, V)
         self.stats.append(st.as_dict())
+        _native.check(rc)
         k = n.value
         out_clips = []
         if clips and k > 0:
@@ -136,10 +209,14 @@ class _Pursuer:
         sl = lab[:k].cpu().numpy().view(np.uint32)
         return si, sl, out_clips
 
+    def close(self):
+        self.up.close()
+
 
 def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
                    kernels_path=None, max_gpu_memory=None, *, mode="fast", device=None,
-                   work_group_size=WORK_GROUP_SIZE, verbose=True, return_stats=False):
+                   work_group_size=WORK_GROUP_SIZE, max_passes=MAX_PASSES, verbose=True,
+                   return_stats=False):
     """Find template spikes in ``voltage`` by binary pursuit on the GPU.
 
     See the module docstring for the contract; the arguments mean what they
@@ -181,17 +258,20 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     if onsets:
         max_chunk = min(n_samples, chunk_len)
         pursuer = _Pursuer(torch, dev, n_chans, templates, bias, theta, W, S, max_chunk, flags,
-                           work_group_size)
-    for start in onsets:
-        stop = int(np.uint32(min(n_samples, start + chunk_len)))
-        host_chunk = np.ascontiguousarray(np.float32(voltage[:, start:stop]))
-        si, sl, clips = pursuer.chunk(host_chunk, get_clips)
-        if si.size == 0:
-            continue
-        idx_all.append(si.astype(np.int64) + start)
-        lab_all.append(sl)
-        clips_all.append(clips)
-        bool_all.append(np.ones(si.size, dtype=bool))
+                           work_group_size, max_passes)
+    try:
+        for start in onsets:
+            stop = int(np.uint32(min(n_samples, start + chunk_len)))
+            si, sl, clips = pursuer.chunk(voltage[:, start:stop], get_clips)
+            if si.size == 0:
+                continue
+            idx_all.append(si.astype(np.int64) + start)
+            lab_all.append(sl)
+            clips_all.append(clips)
+            bool_all.append(np.ones(si.size, dtype=bool))
+    finally:
+        if pursuer is not None:
+            pursuer.close()
     if idx_all:
         event_indices = np.int64(np.hstack(idx_all))
         neuron_labels = np.int64(np.hstack(lab_all))

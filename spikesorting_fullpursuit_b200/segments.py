@@ -32,7 +32,7 @@ def shard_segments(lengths: Sequence[int], world_size: int) -> List[List[int]]:
     return shards
 
 
-def _run_local(segments, mine, lengths, pursue, streams, kwargs):
+def _run_local(segments, mine, lengths, pursue, streams, kwargs, pursue_is_default=False):
     """Results of this rank's segments, by segment index.  With streams > 1 the
     segments (longest first) are taken by that many worker threads; on a CUDA
     device each worker issues its segments on a stream of its own, so several
@@ -47,6 +47,13 @@ def _run_local(segments, mine, lengths, pursue, streams, kwargs):
 
     use_cuda = torch.cuda.is_available()
     device = torch.cuda.current_device() if use_cuda else None
+    if use_cuda and pursue_is_default and kwargs.get("max_gpu_memory") is None:
+        # each concurrent pursuit plans its chunks for a share of the device budget
+        # the reference uses for one (binary_pursuit_parallel.py:389-408), so the
+        # workers together stay within it
+        total = torch.cuda.get_device_properties(device).total_memory
+        budget = max(0.5 * total, total - (1 << 30))
+        kwargs = dict(kwargs, max_gpu_memory=budget / min(streams, len(mine)))
     todo = queue.Queue()
     for i in sorted(mine, key=lambda k: (-lengths[k], k)):
         todo.put(i)
@@ -88,19 +95,24 @@ def pursue_segments(segments, pursue: Callable = None, group=None, streams: int 
     segments: sequence of argument tuples for ``pursue`` (by default the
     drop-in binary_pursuit: (voltage, v_dtype, sort_info, separability_metrics)).
     streams: segments of one rank pursued at once (worker threads, one CUDA
-    stream each); 1 runs them one after another.
+    stream each); 1 runs them one after another.  With the default pursuit and
+    no ``max_gpu_memory``, each worker plans its chunks for 1/streams of the
+    device budget; a segment longer than that share is then chunked where a
+    sequential run would not chunk it (chunk boundaries, and the duplicates the
+    reference leaves in chunk overlaps, follow the budget).
     Returns the list of results in segment order on every rank.  Without an
     initialised process group everything runs locally."""
     import torch.distributed as dist
 
-    if pursue is None:
+    default = pursue is None
+    if default:
         from .overlap.binary_pursuit_parallel import binary_pursuit as pursue
     dist_on = dist.is_available() and dist.is_initialized()
     world = dist.get_world_size(group) if dist_on else 1
     rank = dist.get_rank(group) if dist_on else 0
     lengths = [int(seg[0].shape[1]) for seg in segments]
     mine = shard_segments(lengths, world)[rank]
-    local = _run_local(segments, mine, lengths, pursue, int(streams), kwargs)
+    local = _run_local(segments, mine, lengths, pursue, int(streams), kwargs, default)
     if not dist_on:
         return [local[i] for i in range(len(segments))]
     gathered = [None] * world

@@ -25,15 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-
-def time_window_to_samples(time_window_s, sampling_rate):
-    """Clip window in samples (spikesorting_fullpursuit/processing/conversions.py:4-39)."""
-    w = list(time_window_s)
-    if w[0] > 0:
-        w[0] *= -1
-    s0 = min(int(round(w[0] * sampling_rate)), 0)
-    s1 = max(int(round(w[1] * sampling_rate)), 1) + 1
-    return [s0, s1], w
+from .processing.conversions import time_window_to_samples
 
 
 def band_noise(rng, n_chans, n_samples, fs, lo=300.0, hi=8000.0):

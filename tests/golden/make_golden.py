@@ -10,8 +10,14 @@ inputs, the call arguments, the four return values, and per chunk: the
 SHA-256 of the first-pass likelihood buffer and of the final residual, and
 the spike count of every pursuit pass.
 
-Usage (needs the reference checkout; runs in this container only):
-    python tests/golden/make_golden.py [case ...]
+Cases with ``config`` are recordings of the benchmark generator
+(``synth.config_recording``): a leading slice of the recording the benchmark
+pursues, or the configuration at a shorter duration.  Large voltages are not
+stored: the file keeps the recipe and the SHA-256 of the voltage, and
+tests/conftest.py regenerates it (seeded) and checks the hash.
+
+Usage (needs the reference checkout; runs where the reference can be read):
+    FBP_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -27,7 +33,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("FBP_REFERENCE_ROOT", "/root/reference")
+REFERENCE = os.environ.get("FBP_REFERENCE_ROOT", os.path.join(os.path.dirname(REPO), "reference"))
 sys.path.insert(0, REPO)
 sys.path.insert(0, os.path.join(REPO, "oracle"))
 
@@ -62,7 +68,35 @@ CASES = {
                             dict(n_max_shift_inds=100), dict(clips=False)),
     "duplicate_template": (dict(seed=19, n_chans=4, duration_s=0.25, n_units=3),
                            dict(n_max_shift_inds=20), dict(clips=True, duplicate=True)),
+    # the benchmark's own recording (16 ch, 40 templates, 10 min), its leading second
+    "linear16_bench_1s": (dict(config="linear16", seed=1, slice_s=1.0),
+                          dict(n_max_shift_inds=100), dict(clips=True, store_voltage=True)),
+    # the tetrode configuration in full: 4 ch, 30 s, 6 templates
+    "tetrode_cfg0_30s": (dict(config="tetrode", seed=1),
+                         dict(n_max_shift_inds=100), dict(clips=False, store_voltage=False)),
+    # the dense 64-channel configuration's 200 templates (76 taps) on 0.1 s
+    "dense64_m200_0p1s": (dict(config="dense64", seed=1, duration_s=0.1),
+                          dict(n_max_shift_inds=75), dict(clips=True, store_voltage=True)),
 }
+
+HEAVY = ("linear16_bench_1s", "tetrode_cfg0_30s", "dense64_m200_0p1s")
+
+
+def make_inputs(rec_kw):
+    """Voltage, sort_info, metrics of a case's recording kwargs (see CASES)."""
+    rec_kw = dict(rec_kw)
+    seed = rec_kw.pop("seed")
+    if "config" not in rec_kw:
+        voltage, sort_info, metrics, _ = synth.make_recording(seed, **rec_kw)
+        return voltage, sort_info, metrics
+    name = rec_kw.pop("config")
+    slice_s = rec_kw.pop("slice_s", None)
+    voltage, sort_info, metrics, _ = synth.config_recording(name, seed, **rec_kw)
+    if slice_s is not None:
+        n = int(round(slice_s * sort_info["sampling_rate"]))
+        voltage = np.ascontiguousarray(voltage[:, :n])
+        sort_info = dict(sort_info, n_samples=n)
+    return voltage, sort_info, metrics
 
 
 def _import_reference():
@@ -83,9 +117,8 @@ def _sha(a: np.ndarray) -> str:
 
 def build_case(name, fcl, bpp, ns):
     rec_kw, call_kw, extra = CASES[name]
-    rec_kw = dict(rec_kw)
-    seed = rec_kw.pop("seed")
-    voltage, sort_info, metrics, truth = synth.make_recording(seed, **rec_kw)
+    seed = rec_kw["seed"]
+    voltage, sort_info, metrics = make_inputs(rec_kw)
     if extra.get("duplicate"):
         T = metrics["templates"].copy()
         T[2] = T[0]
@@ -166,9 +199,11 @@ def build_case(name, fcl, bpp, ns):
     }
     for ch in meta["chunks"]:
         ch.setdefault("resid_sha256", None)
+    meta["voltage_sha256"] = _sha(np.float32(voltage))
+    stored = {"voltage": voltage} if extra.get("store_voltage", True) else {}
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"),
-        voltage=voltage,
+        **stored,
         templates=np.asarray(metrics["templates"]),
         template_SS=np.asarray(metrics["template_SS"]),
         template_SS_by_chan=np.asarray(metrics["template_SS_by_chan"]),

@@ -74,3 +74,23 @@ def test_noalloc_rejects_more_spikes_than_its_array():
                                 _native.NOALLOC_MAX_SPIKES + 1, None)
     assert rc == _native.FBP_E_ARG
     assert b"FBP_NOALLOC_MAX_SPIKES" in L.fbp_last_error()
+
+
+def test_noalloc_clears_the_previous_error():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    L = _native.lib()
+    V, T, idx, lab, W = _inputs(3, N=20000, n=50)
+    d = _native.dims(V.shape[0], V.shape[1], T.shape[0], W, 10)
+    Vd, Td = torch.from_numpy(V).cuda(), torch.from_numpy(T).cuda()
+    idd = torch.from_numpy(idx.view(np.int32)).cuda()
+    ld = torch.from_numpy(lab.view(np.int32)).cuda()
+    # more spikes than the chunk has windows: rejected like fbp_residual rejects it
+    nw = (V.shape[1] + W - 1) // W
+    many = torch.zeros(nw + 1, dtype=torch.int32, device="cuda")
+    assert L.fbp_residual_noalloc(ctypes.byref(d), _ptr(Vd), _ptr(Td), _ptr(many), _ptr(many), nw + 1,
+                                  None) == _native.FBP_E_ARG
+    assert L.fbp_last_error() != b""
+    _native.check(L.fbp_residual_noalloc(ctypes.byref(d), _ptr(Vd), _ptr(Td), _ptr(idd), _ptr(ld), idx.size, None))
+    torch.cuda.synchronize()
+    assert L.fbp_last_error() == b""
