@@ -133,26 +133,34 @@ def load_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def leading_slice(V, si, seconds):
+    """The first `seconds` of a recording (same templates and thresholds)."""
+    n = min(V.shape[1], max(si["n_samples_per_chan"] + 1, int(round(seconds * si["sampling_rate"]))))
+    return np.ascontiguousarray(V[:, :n]), dict(si, n_samples=n)
+
+
 def run_reference(args, rank):
-    """The reference kernels on the host cores, bounded slice of the workload."""
+    """The reference kernels on the host cores, on a bounded leading slice of
+    the same recording the other arm pursues (same seed, templates, thresholds)."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(HERE, "oracle"))
     from spikesorting_fullpursuit_b200 import synth
     import ref_host
-    # warm-up steps load the library and touch the code path on a short slice; the timed
+    Vfull, sifull, sm, _ = synth.config_recording(args.config, seed=1, duration_s=args.duration)
+    # warm-up steps load the library and touch the code path on a 0.1 s slice; the timed
     # slice is sized from the warm-up rate so that the K timed steps take about 150 s
-    Vw, siw, smw, _ = synth.config_recording(args.config, seed=1, duration_s=0.1)
+    Vw, siw = leading_slice(Vfull, sifull, 0.1)
     Ww = siw["n_samples_per_chan"]
     rate = None
     for _ in range(args.warmup):
         t0 = time.perf_counter()
-        ref_host.binary_pursuit(Vw, siw, copy.deepcopy(smw), n_max_shift_inds=Ww - 1)
+        ref_host.binary_pursuit(Vw, siw, copy.deepcopy(sm), n_max_shift_inds=Ww - 1)
         rate = Vw.shape[1] / (time.perf_counter() - t0)   # samples per second
     sample_s = args.cpu_sample_s
     if rate:
         sample_s = float(np.clip(150.0 / max(1, args.steps) * rate / siw["sampling_rate"], 0.25, args.cpu_sample_s))
-    V, si, sm, _ = synth.config_recording(args.config, seed=1, duration_s=sample_s)
+    V, si = leading_slice(Vfull, sifull, sample_s)
     W = si["n_samples_per_chan"]
     times = []
     for _ in range(args.steps):
@@ -167,9 +175,9 @@ def run_reference(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": "%s (leading %.1f s slice)" % (args.config, sample_s)},
+        "config": {"workload": "%s (leading %.2f s slice of the seed-1 recording)" % (args.config, sample_s)},
         "cpu_baseline": {"value": value, "unit": "Msample*ch/s", "cores": cores, "kind": "reference",
-                         "sample": "leading %.1f s of the %s recording, %d channels, reference OpenCL "
+                         "sample": "leading %.2f s of the %s recording (seed 1), %d channels, reference OpenCL "
                                    "kernels compiled for the CPU, host loop restated" %
                                    (sample_s, args.config, V.shape[0])},
         "e2e": {"value": value, "unit": "Msample*ch/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -299,7 +307,8 @@ def main():
     if not args.no_plain and plain_work > 1e10:
         plain = {"skipped": "brute-force recheck of %.1e multiply-adds per flagged window" % plain_work}
     elif not args.no_plain:
-        ms_plain, st_plain, res_plain = run_mode(_native.FBP_PLAIN_FP32, 1, 1)
+        ms_plain, _, res_plain = run_mode(_native.FBP_PLAIN_FP32, 1, 1)
+        _, st_plain, _ = run_mode(_native.FBP_PLAIN_FP32, 1, 0, timing=True)   # stage times (serialised)
         a = set(zip(res_fast[0].tolist(), res_fast[1].tolist()))
         b = set(zip(res_plain[0].tolist(), res_plain[1].tolist()))
         match = len(a & b) / max(1, len(a | b))
@@ -314,27 +323,41 @@ def main():
     # algorithmic work each kernel family does in that step
     S2 = 2 * S + 1
     listed, flagged = st_stage["listed"], st_stage["flagged"]
+    # FP32 FMA issue peak of the SIMT pipes (148 SMs x 128 lanes x 2 flop) at the
+    # median SM clock of the timed region (nominal max clock if no sample)
+    fma_peak = 148 * 128 * 2 * (clocks.get("sm_mhz") or 1965.0) * 1e6 / 1e12
     fam = {
-        "lik_tc_kernel": (st_stage["ms_lik_tc"], "tensor", 2.0 * M * C * W * W * listed),
-        "fixup_kernel": (st_stage["ms_fixup"], "fp32", 2.0 * C * W * 4 * st_stage["fixup_runs_queued"]),
-        "partial_corr_kernel": (st_stage["ms_partial_corr"], "fp32", 2.0 * M * C * W * S2 * flagged),
-        "screen_kernel": (st_stage["ms_screen"], "hbm", (4.0 * C * W + 8.0 * M * S2 + 4.0 * M * S2) * flagged),
-        "score_kernel": (st_stage["ms_score"], "fp32", 5.0 * C * W * st_stage["pair_exact"]),
-        "argmax_kernel": (st_stage["ms_argmax"], "hbm", 12.0 * M * W * listed + 22.0 * listed),
+        "lik_tc_kernel": (st_stage["ms_lik_tc"], "tensor", 2.0 * M * C * W * W * listed,
+                          "2*M*C*W*W flop per listed window (nominal dense product)"),
+        "fixup_kernel": (st_stage["ms_fixup"], "fp32", 2.0 * C * W * 4 * st_stage["fixup_runs_queued"],
+                         "2*C*W flop per sample recomputed"),
+        "partial_corr_kernel": (st_stage["ms_partial_corr"], "fp32", 2.0 * st_stage["pc_macs"],
+                                "2 flop per multiply-add done (device counter)"),
+        "screen_kernel": (st_stage["ms_screen"], "latency", None, "L2-latency-bound table scan"),
+        "score_kernel": (st_stage["ms_score"], "latency", None, "one sequential C*W chain per candidate"),
+        "argmax_kernel": (st_stage["ms_argmax"], "hbm", 24.0 * listed, "3 window keys (8 B) per listed window"),
     }
     kernels = {}
-    for name, (ms, bound, work) in fam.items():
+    for name, (ms, bound, work, what) in fam.items():
         if ms <= 0:
             continue
-        if bound == "hbm":
+        if bound == "latency":
+            kernels[name] = {"ms": ms, "bound": "latency", "note": what}
+        elif bound == "hbm":
             ach = work / (ms * 1e-3) / 1e9
             kernels[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                             "frac": ach / hbm}
+                             "frac": ach / hbm, "work": what}
+        elif bound == "tensor":
+            ach = work / (ms * 1e-3) / 1e12
+            kernels[name] = {"ms": ms, "bound": "tensor", "achieved": ach, "peak": tflops, "unit": "TFLOP/s",
+                             "frac": ach / tflops, "work": what}
         else:
             ach = work / (ms * 1e-3) / 1e12
-            kernels[name] = {"ms": ms, "bound": "tensor" if bound == "tensor" else "fp32-simt",
-                             "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops}
-    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+            kernels[name] = {"ms": ms, "bound": "fp32-simt", "achieved": ach, "peak": fma_peak,
+                             "unit": "TFLOP/s", "frac": ach / fma_peak, "work": what,
+                             "peak_kind": "nominal FP32 FMA issue rate at the sampled clock"}
+    # the roofline line reports the dominant kernel among those with a throughput bound
+    dom = max((k for k in kernels if kernels[k]["bound"] != "latency"), key=lambda k: kernels[k]["ms"])
     roof = dict(kernels[dom])
     # DRAM bytes (read + write) per launch: ncu's per-unit figure from the captures in
     # profiles/ (60 s slice of this workload) times the units of an average launch here
@@ -351,7 +374,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args)
+        cpu = cpu_baseline(args, V, si, sm)
 
     if rank == 0:
         line = {
@@ -370,7 +393,8 @@ def main():
             "gpu_launches": launches,
             "stages_ms": {k[3:]: v for k, v in st_stage.items() if k.startswith("ms_") and v > 0},
             "kernels": kernels,
-            "stats": {k: st_stage[k] for k in ("passes", "n_spikes", "listed", "flagged", "fixups", "fixup_runs_queued", "pair_exact")},
+            "stats": {k: st_stage[k] for k in ("passes", "n_spikes", "listed", "flagged", "fixups", "fixup_runs_queued",
+                                               "pair_exact", "pc_macs", "pass_spikes")},
             "roofline": roof,
             "plain_fp32": plain,
             "cpu_baseline": cpu,
@@ -435,11 +459,13 @@ def run_adjoint(args):
                                                                                    si["sampling_rate"], M, W, n)}}))
 
 
-def cpu_baseline(args):
+def cpu_baseline(args, Vfull, sifull, sm):
+    """The reference kernels on the host cores over the leading slice of the
+    benchmark's own recording (the --impl reference arm times the same code on
+    the same slice)."""
     sys.path.insert(0, os.path.join(HERE, "oracle"))
-    from spikesorting_fullpursuit_b200 import synth
     sample_s = args.cpu_sample_s
-    V, si, sm, _ = synth.config_recording(args.config, seed=1, duration_s=sample_s)
+    V, si = leading_slice(Vfull, sifull, sample_s)
     W = si["n_samples_per_chan"]
     try:
         import ref_host
@@ -458,7 +484,7 @@ def cpu_baseline(args):
         cores = os.cpu_count()
         what = "C restatement (oracle) with OpenMP"
     return {"value": V.shape[0] * V.shape[1] / dt / 1e6, "unit": "Msample*ch/s", "cores": cores,
-            "kind": kind, "sample": "leading %.1f s of the %s recording (%d ch); %s" % (
+            "kind": kind, "sample": "leading %.2f s of the benchmark's %s recording (seed 1, %d ch); %s" % (
                 sample_s, args.config, V.shape[0], what)}
 
 

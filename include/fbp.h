@@ -79,6 +79,7 @@ typedef struct fbp_chunk_stats {
     uint32_t fixup_runs_queued; /* runs recomputed by the separate fixup kernel (the others inside
                                    the likelihood kernel, from its staged voltage) */
     uint64_t launches;       /* kernels launched by the call */
+    uint64_t pc_macs;        /* multiply-adds the screened recheck's partial correlations did */
     /* spikes added by each pass: pass p (1-based) at [(p - 1) % FBP_PASS_RING], so
        after more than FBP_PASS_RING passes the ring holds the most recent ones */
     uint32_t pass_spikes[FBP_PASS_RING];
@@ -195,6 +196,28 @@ int fbp_adjoint_grad(const fbp_dims* dims, const float* voltage, const float* te
                      const uint32_t* spike_idx, const uint32_t* spike_lab, const float* amplitude,
                      const float* shift, uint32_t n_spikes, double scale, double* grad_templates64,
                      float* grad_templates, float* grad_amplitude, float* grad_shift, void* stream);
+
+/* ---- post-pursuit duplicate removal (device-resident output) ---- */
+
+/* Mean clip of one unit, np.mean(clips, axis=0) in float32 (rows summed in
+ * order, then divided by n): the template WorkItemSummary.
+ * remove_segment_binary_pursuit_duplicates passes
+ * (spikesorting_fullpursuit/postprocessing.py:660-666).  clips float32 [n][clip_len]. */
+int fbp_mean_clip(const float* clips, uint32_t n, uint32_t clip_len, float* mean, void* stream);
+
+/* Device workspace bytes fbp_bp_duplicates needs for n spikes. */
+size_t fbp_bp_duplicates_workspace(uint32_t n);
+
+/* remove_binary_pursuit_duplicates (spikesorting_fullpursuit/analyze_spike_timing.py:148-193)
+ * for the spikes of one unit: keep[i] = 0 where spike i is dropped.  Of two spikes
+ * within tol_inds samples that binary pursuit both found (bp != 0), the one whose
+ * clip has the larger float32 sum of squared differences from unit_template
+ * (numpy's pairwise summation order) is dropped, walking the spikes in the given
+ * order exactly as the reference does.  event_indices int64 [n], clips float32
+ * [n][clip_len], unit_template float32 [clip_len], bp uint8 [n], keep uint8 [n]. */
+int fbp_bp_duplicates(const int64_t* event_indices, const float* clips, const float* unit_template,
+                      const uint8_t* bp, uint32_t n, uint32_t clip_len, int64_t tol_inds,
+                      uint8_t* keep, void* workspace, size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -26,7 +26,8 @@ FBP_TIMING = 0x4
 # every function include/fbp.h declares
 EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_pursue_chunk",
            "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc",
-           "fbp_adjoint_loss", "fbp_adjoint_grad")
+           "fbp_adjoint_loss", "fbp_adjoint_grad", "fbp_mean_clip", "fbp_bp_duplicates_workspace",
+           "fbp_bp_duplicates")
 NOALLOC_MAX_SPIKES = 65536
 PASS_RING = 64
 ABI_VERSION = 3
@@ -49,7 +50,8 @@ class FbpChunkStats(ctypes.Structure):
                 ("ms_lik_exact", ctypes.c_float), ("ms_partial_corr", ctypes.c_float),
                 ("ms_screen", ctypes.c_float), ("ms_score", ctypes.c_float),
                 ("ms_overlap_plain", ctypes.c_float), ("fixup_runs_queued", ctypes.c_uint32),
-                ("launches", ctypes.c_uint64), ("pass_spikes", ctypes.c_uint32 * PASS_RING)]
+                ("launches", ctypes.c_uint64), ("pc_macs", ctypes.c_uint64),
+                ("pass_spikes", ctypes.c_uint32 * PASS_RING)]
 
     def as_dict(self):
         out = {k: getattr(self, k) for k, _ in self._fields_}
@@ -101,6 +103,12 @@ def lib():
     L.fbp_adjoint_loss.restype = ctypes.c_int
     L.fbp_adjoint_grad.argtypes = [P(FbpDims), vp, vp, vp, vp, vp, vp, u32, ctypes.c_double, vp, vp, vp, vp, vp]
     L.fbp_adjoint_grad.restype = ctypes.c_int
+    L.fbp_mean_clip.argtypes = [vp, u32, u32, vp, vp]
+    L.fbp_mean_clip.restype = ctypes.c_int
+    L.fbp_bp_duplicates_workspace.argtypes = [u32]
+    L.fbp_bp_duplicates_workspace.restype = sz
+    L.fbp_bp_duplicates.argtypes = [vp, vp, vp, vp, u32, u32, ctypes.c_int64, vp, vp, sz, vp]
+    L.fbp_bp_duplicates.restype = ctypes.c_int
     _lib = L
     return L
 

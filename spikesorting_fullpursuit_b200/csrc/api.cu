@@ -115,6 +115,10 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
         if (cap > (32ull << 20)) cap = 32ull << 20;
         L->n_fix_cap = cap + 4096;
         L->off_fix = take(L->n_fix_cap * 8);
+        L->nwb = (N + 31) / 32 + 1;
+        L->off_wkey = take(nw * 8);
+        L->off_wpos = take(nw);
+        L->off_inexact = take(M * L->nwb * 4);
     }
     if (!(flags & FBP_PLAIN_FP32) && (flags & FBP_OVERLAP_RECHECK)) {
         const uint64_t xt = M * M * S2 * S2 * 4;
@@ -213,6 +217,9 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     const bool overlap = (flags & FBP_OVERLAP_RECHECK) != 0;
     const bool timing = (flags & 0x4u) != 0;
     const bool use_tc = !plain && tc_supported(dims_of(lay));
+    // tensor-core likelihood with lazy exactness: estimates kept where no
+    // decision needs the exact value (see lik_tc.cu)
+    const bool lazy = use_tc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     fbp_chunk_stats local{};
     fbp_chunk_stats& S = stats ? *stats : local;
@@ -239,6 +246,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         FBP_TRY(launch_tc_prepare_templates(d, w, templates, st));
         FBP_TRY(launch_tc_update_voltage(d, w, voltage, nullptr, nullptr, 0, true, st));
     }
+    if (lazy) FBP_CUDA(cudaMemsetAsync(w.base + lay.off_inexact, 0, lay.M * lay.nwb * 4, st));
     if (!plain && overlap) FBP_TRY(launch_overlap_tables(d, w, templates, st));
     uint32_t nlist = d.nw, total = 0;
     api_detail::StageTimer tm;
@@ -256,13 +264,16 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         tm.start(timing, st, &S.ms_likelihood);
         if (use_tc) {
             uint64_t nfix = 0;
-            FBP_TRY(launch_likelihood_tc(d, w, voltage, templates, bias, w.list(), nlist, w.L(), false, st, &nfix));
+            FBP_TRY(launch_likelihood_tc(d, w, voltage, templates, bias, w.list(), nlist, w.L(), lazy, st, &nfix));
         } else {
             FBP_TRY(launch_likelihood_exact(d, voltage, templates, bias, w.list(), nlist, w.L(), st));
         }
         tm.stop();
         tm.start(timing, st, &S.ms_argmax);
-        FBP_TRY(launch_argmax(d, w, w.list(), nlist, st));
+        if (lazy)
+            FBP_TRY(launch_argmax_lazy(d, w, w.list(), nlist, st));
+        else
+            FBP_TRY(launch_argmax(d, w, w.list(), nlist, st));
         tm.stop();
         tm.start(timing, st, &S.ms_overlap);
         if (overlap) {
@@ -271,11 +282,12 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
                 FBP_TRY(launch_overlap_plain(d, w, voltage, templates, theta, nlist, st));
             else
                 FBP_TRY(launch_overlap_fast(d, w, voltage, templates, theta, nlist, st));
-            FBP_TRY(launch_parse_reassign(d, w, theta, nlist, st));
+            FBP_TRY(launch_parse_reassign(d, w, theta, nlist, st, voltage, templates, bias, lazy));
         }
         tm.stop();
         tm.start(timing, st, &S.ms_accept);
         FBP_TRY(launch_accept(d, w, theta, nlist, st));
+        if (lazy) FBP_TRY(launch_lazy_fix(d, w, voltage, templates, bias, nlist, st));
         FBP_TRY(launch_next_list(d, w, st));
         tm.stop();
         DevStatus hs;
@@ -316,6 +328,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     FBP_CUDA(cudaStreamSynchronize(st));
     S.pair_exact = (plain || !lay.screened) ? hs.pair_items : hs.n_pair_exact;
     S.fixups += 4ull * hs.n_fix_local;
+    S.pc_macs = hs.pc_macs;
     S.n_spikes = total;
     S.launches = kclock().launches;
     *n_spikes = total;

@@ -63,6 +63,7 @@ struct DevStatus {
     unsigned long long pair_items;  // items evaluated by the overlap recheck
     uint32_t cand_count;    // candidates appended to the exact-scoring list (per batch)
     uint32_t n_fix_local;   // runs recomputed inside the likelihood kernel (whole call)
+    unsigned long long pc_macs;   // multiply-adds done by the partial correlations (whole call)
 };
 
 // ---------------------------------------------------------------------------
@@ -77,6 +78,10 @@ struct Layout {
     // tensor-core likelihood (mode 1)
     size_t off_vt_hi, off_tt_hi, off_tpad, off_fix, off_tnorm;
     uint64_t Cp, Mp, n_fix_cap, vq_rows;
+    // lazy exactness of the tensor-core likelihood: per-window maximum keys and
+    // positive flags, one "estimate" bit per likelihood sample ([M][nwb] words)
+    size_t off_wkey, off_wpos, off_inexact;
+    uint64_t nwb;
     // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
     // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
     // template processing order perm[M]
@@ -117,6 +122,16 @@ struct Work {
     DevStatus* status() const { return at<DevStatus>(lay->off_status); }
 };
 
+// Where the tensor-core likelihood left estimates (lazy exactness): readers of
+// a likelihood value recompute it exactly when its bit is set.
+struct LazyRef {
+    const uint32_t* inexact;   // [M][nwb] bits, or null: L is exact wherever read
+    uint32_t nwb;
+    const float* V;
+    const float* T;
+    const float* bias;
+};
+
 // Sizes passed by value to kernels.
 struct Dims {
     uint32_t C, N, M, W, S, WG, nw, nwf;
@@ -140,7 +155,8 @@ int launch_compact_flagged(const Dims& d, const Work& w, uint32_t nlist, cudaStr
 int launch_overlap_plain(const Dims& d, const Work& w, const float* V, const float* T,
                          const float* theta, uint32_t nflag_max, cudaStream_t st);
 int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint32_t nflag_max,
-                          cudaStream_t st);
+                          cudaStream_t st, const float* V = nullptr, const float* T = nullptr,
+                          const float* bias = nullptr, bool lazy = false);
 int launch_accept(const Dims& d, const Work& w, const float* theta, uint32_t nlist,
                   cudaStream_t st);
 int launch_next_list(const Dims& d, const Work& w, cudaStream_t st);
@@ -154,7 +170,13 @@ int launch_adjusted_clips(const Dims& d, const float* V, const float* T, const u
 bool tc_supported(const Dims& d);
 int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T,
                          const float* bias, const uint32_t* list, uint32_t nlist, float* L,
-                         bool refresh_voltage, cudaStream_t st, uint64_t* n_fix_out);
+                         bool lazy, cudaStream_t st, uint64_t* n_fix_out);
+// Lazy exactness: per-window argmax from the window keys, and the exact
+// recomputation of estimates whose voltage the coming residual changes in
+// windows the next pass does not relist.
+int launch_argmax_lazy(const Dims& d, const Work& w, const uint32_t* list, uint32_t nlist, cudaStream_t st);
+int launch_lazy_fix(const Dims& d, const Work& w, const float* V, const float* T, const float* bias,
+                    uint32_t nmax, cudaStream_t st);
 int launch_tc_prepare_templates(const Dims& d, const Work& w, const float* T, cudaStream_t st);
 int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const uint32_t* idx,
                              const uint32_t* win, uint32_t n, bool all, cudaStream_t st);

@@ -480,11 +480,35 @@ __global__ void __launch_bounds__(kOvThreads) overlap_plain_kernel(
 // parse_overlap_recheck_indices (binary_pursuit.cl:657-815), one thread per
 // flagged window, from the winner key.
 // ---------------------------------------------------------------------------
+// Exact likelihood of (t, s) in the reference order (compute_maximum_likelihood,
+// binary_pursuit.cl:216-252) from the current voltage.
+__device__ float exact_lik(const Dims& d, const float* __restrict__ V, const float* __restrict__ T, float b,
+                           uint32_t t, uint32_t s)
+{
+    float acc = b;
+    for (uint32_t c = 0; c < d.C; ++c) {
+        const float* tr = T + ((uint64_t)t * d.C + c) * d.W;
+        const float* vr = V + (uint64_t)c * d.N + s;
+        for (uint32_t j = 0; j < d.W; ++j) acc = fadd(acc, fmul(tr[j], vr[j]));
+    }
+    return acc;
+}
+
+// L[t][s], made exact where the tensor-core likelihood left an estimate (its
+// voltage is unchanged since, so the current voltage gives the exact value).
+__device__ __forceinline__ float lik_value(const Dims& d, const float* __restrict__ L, const LazyRef& z, uint32_t t,
+                                           uint32_t s)
+{
+    if (z.inexact != nullptr && ((z.inexact[(uint64_t)t * z.nwb + (s >> 5)] >> (s & 31u)) & 1u))
+        return exact_lik(d, z.V, z.T, z.bias[t], t, s);
+    return L[(uint64_t)t * d.N + s];
+}
+
 __global__ void parse_kernel(Dims d, const float* __restrict__ L, const float* __restrict__ theta,
                              const uint32_t* __restrict__ flag, const DevStatus* status,
                              const unsigned long long* __restrict__ keys, float* best_lik,
                              const uint32_t* __restrict__ best_lab, const uint32_t* __restrict__ best_idx,
-                             uint8_t* orech, uint32_t* ov_idx, uint32_t* ov_lab)
+                             uint8_t* orech, uint32_t* ov_idx, uint32_t* ov_lab, LazyRef z)
 {
     const uint32_t nflag = status->n_flag;
     const uint64_t S2 = 2ull * d.S + 1;
@@ -507,8 +531,8 @@ __global__ void parse_kernel(Dims d, const float* __restrict__ L, const float* _
         const uint32_t t = (uint32_t)(r % d.M);
         const uint64_t a = (r / d.M) % S2, b = (r / (S2 * d.M)) % S2;
         const uint32_t afi = (uint32_t)(p + a - d.S), asi = (uint32_t)(p + b - d.S);
-        const float l1 = L[(uint64_t)f * d.N + afi];
-        const float l2 = L[(uint64_t)t * d.N + asi];
+        const float l1 = lik_value(d, L, z, f, afi);
+        const float l2 = lik_value(d, L, z, t, asi);
         if (gv < l1 || gv < l2) { orech[id] = 0; continue; }
         if (l1 <= 0.f || l2 <= 0.f) { orech[id] = 0; continue; }
         if (l1 >= l2 && l1 > theta[f]) { best_lik[id] = l1; ov_lab[id] = f; ov_idx[id] = afi; }
@@ -931,13 +955,19 @@ int launch_overlap_plain(const Dims& d, const Work& w, const float* V, const flo
     return FBP_OK;
 }
 
-int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint32_t nflag_max, cudaStream_t st)
+int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint32_t nflag_max, cudaStream_t st,
+                          const float* V, const float* T, const float* bias, bool lazy)
 {
     if (nflag_max == 0) return FBP_OK;
     const uint32_t g = grid_for(nflag_max, 256);
+    LazyRef z{nullptr, 0, V, T, bias};
+    if (lazy) {
+        z.inexact = w.at<uint32_t>(w.lay->off_inexact);
+        z.nwb = (uint32_t)w.lay->nwb;
+    }
     count_launch(5);
     parse_kernel<<<g, 256, 0, st>>>(d, w.L(), theta, w.flag(), w.status(), w.keys(), w.best_lik(),
-                                    w.best_lab(), w.best_idx(), w.orech(), w.ov_idx(), w.ov_lab());
+                                    w.best_lab(), w.best_idx(), w.orech(), w.ov_idx(), w.ov_lab(), z);
     reassign_resolve_kernel<<<g, 256, 0, st>>>(d, w.flag(), w.status(), w.orech(), w.ov_idx(), w.orech_fin());
     reassign_apply_kernel<<<g, 256, 0, st>>>(d, w.flag(), w.status(), w.orech(), w.orech_fin(), w.best_idx(),
                                              w.best_lab(), w.check(), w.ov_idx(), w.ov_lab());

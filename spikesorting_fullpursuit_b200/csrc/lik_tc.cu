@@ -43,6 +43,7 @@ constexpr int kTile = 128;         // samples per UMMA tile (M)
 constexpr int kThreads = 192;
 constexpr uint64_t kWaitNs = 250ull * 1000ull * 1000ull;   // longest mbarrier wait (global timer)
 constexpr uint32_t kFixCap = 1024;   // runs recomputed in the CTA itself; more go to the global queue
+constexpr uint32_t kWinSlots = 130;  // windows one 128-sample tile can touch (W >= 1)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -161,7 +162,24 @@ struct TcParams {
     uint32_t fix_cap;
     DevStatus* status;
     float k_a, k_b;       // bound = k_a * sum_c |T_tc| |V_c strip| + k_b * |bias_t|
+    // lazy exactness (pursuit): only samples whose sign is uncertain and the
+    // contenders for each window's maximum are recomputed exactly; every other
+    // positive sample keeps its estimate and its bit in `inexact` is set
+    uint32_t lazy;
+    unsigned long long* wkey;   // [nw] window maximum: see window_key()
+    uint8_t* wpos;              // [nw] 1 if the window holds a positive likelihood
+    uint32_t* inexact;          // [M][nwb] one bit per sample: L holds an estimate
+    uint32_t nwb;               // 32-bit words per template row of `inexact`
 };
+
+// Key of a positive likelihood v at (template t, sample s) of window w:
+// larger for a larger value, then for a smaller t, then for a smaller s -- the
+// order in which compute_template_maximum_likelihood (binary_pursuit.cl:395-408)
+// keeps the first maximum.  Needs W <= 1024 and t < 2^22.
+__device__ __forceinline__ unsigned long long window_key(float v, uint32_t t, uint32_t local_s)
+{
+    return ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - ((t << 10) | local_s));
+}
 
 __device__ float exact_likelihood(const Dims& d, const float* __restrict__ V, const float* __restrict__ T,
                                   float b, uint32_t t, uint32_t s)
@@ -200,6 +218,11 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
     float* sbias = bnd + P.ntiles * d.M;                          // [M]
     uint32_t* fq = reinterpret_cast<uint32_t*>(sbias + d.M);      // [kFixCap] runs: t | tile | row | mask
     uint32_t* nfq = fq + kFixCap;
+    uint32_t* t_w0 = nfq + 1;                                      // [ntiles] first window of each tile
+    int* s_mlb = reinterpret_cast<int*>(t_w0 + P.ntiles);          // [ntiles][kWinSlots] max lower bound (float bits)
+    uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_mlb + P.ntiles * kWinSlots);   // [ntiles][kWinSlots]
+    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(
+        (reinterpret_cast<uintptr_t>(s_pos + P.ntiles * kWinSlots) + 7) & ~(uintptr_t)7);   // [ntiles][kWinSlots]
 
     const uint32_t ksteps = d.W * (P.Cq / 2);
     const uint32_t ngroups = (ksteps + P.group - 1) / P.group;
@@ -227,6 +250,12 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         }
         t_s0[i] = s0;
         t_rows[i] = rows;
+        t_w0[i] = s0 / d.W;
+    }
+    for (uint32_t e = threadIdx.x; e < P.ntiles * kWinSlots; e += blockDim.x) {
+        s_mlb[e] = 0;
+        s_pos[e] = 0;
+        s_key[e] = 0ull;
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -312,9 +341,56 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         } else {
             const uint32_t qd = warp & 3;
             const uint32_t row = qd * 32 + lane;
+            // Queue the warp's samples flagged by `need` (template t, tile i) for an
+            // exact recomputation, as runs of 4 consecutive rows (one entry per
+            // non-empty nibble of the ballot): first into this CTA's own list
+            // (recomputed below from the staged strips), then the global queue
+            // (fixup_kernel), else right here.  Returns the sample's exact value if
+            // it was computed here, else `out` unchanged.
+            auto enqueue = [&](bool need, uint32_t t, uint32_t i, uint32_t s, float b, float out, bool& inline_done) {
+                inline_done = false;
+                const uint32_t m = __ballot_sync(0xffffffffu, need);
+                if (m == 0u) return out;
+                uint32_t nz = 0;   // bit k: nibble k non-empty
+#pragma unroll
+                for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                const uint32_t k = lane >> 2;
+                const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
+                const uint32_t nib = (m >> (4 * k)) & 0xFu;
+                const bool local = nib && slot < kFixCap;
+                if ((lane & 3u) == 0 && local) fq[slot] = (t << 13) | (i << 11) | (row << 4) | nib;
+                const bool glob = nib && !local;
+                uint32_t g = 0;
+                if (glob && (lane & 3u) == 0) {
+                    g = atomicAdd(&P.status->n_fix, 1u);
+                    if (g < P.fix_cap)
+                        P.fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | s;
+                }
+                g = __shfl_sync(0xffffffffu, g, lane & ~3u);   // all lanes: the run's first lane holds g
+                const bool queued = local || (glob && g < P.fix_cap);
+                if (need && !queued) {
+                    inline_done = true;
+                    return exact_likelihood(d, P.V, P.T, b, t, s);
+                }
+                return out;
+            };
+            // exact positive value v at (t, s) of tile i: window maximum and sign
+            auto note_exact = [&](float v, uint32_t t, uint32_t i, uint32_t s) {
+                if (!(v > 0.f)) return;
+                const uint32_t w = s / d.W, slot = i * kWinSlots + (w - t_w0[i]);
+                atomicMax(&s_key[slot], window_key(v, t, s - w * d.W));
+                s_pos[slot] = 1u;
+            };
+            // pass 1: estimates, bounds, samples of uncertain sign (lazy) or every
+            // sample that can be positive (not lazy)
             for (uint32_t i = 0; i < P.ntiles; ++i) {
                 const uint32_t s = t_s0[i] + row;
                 const bool valid = row < t_rows[i];
+                const bool live = valid && (uint64_t)s + d.W < d.N;
+                const uint32_t wslot = valid ? i * kWinSlots + (s / d.W - t_w0[i]) : 0u;
                 for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
                     float v[16];
                     tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
@@ -322,44 +398,65 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
                     for (int e = 0; e < 16; ++e) {
                         const uint32_t t = cg * 16 + e;
                         if (t >= d.M) continue;   // uniform over the warp
-                        const bool live = valid && (uint64_t)s + d.W < d.N;
                         const float b = sbias[t];
                         const float est = v[e] + b;
-                        const bool need = live && !(est + bnd[i * d.M + t] <= 0.f);
-                        // queue the warp's samples needing an exact value as runs of 4
-                        // consecutive rows (one entry per non-empty nibble of the ballot)
-                        const uint32_t m = __ballot_sync(0xffffffffu, need);
-                        if (m == 0u) {
-                            if (valid) P.L[(uint64_t)t * d.N + s] = live ? est : 0.f;
-                            continue;
+                        const float bd = bnd[i * d.M + t];
+                        const bool certain = P.lazy && live && est - bd > 0.f;
+                        const bool need = live && !(est + bd <= 0.f) && !certain;
+                        if (certain) {
+                            atomicMax(&s_mlb[wslot], __float_as_int(est - bd));
+                            s_pos[wslot] = 1u;
                         }
-                        uint32_t nz = 0;   // bit k: nibble k non-empty
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
-                        // first into this CTA's own list (recomputed below from the staged
-                        // strips), then the global queue, then inline
-                        uint32_t base = 0;
-                        if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
-                        base = __shfl_sync(0xffffffffu, base, 0);
-                        const uint32_t k = lane >> 2;
-                        const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
-                        const uint32_t nib = (m >> (4 * k)) & 0xFu;
-                        const bool local = nib && slot < kFixCap;
-                        if ((lane & 3u) == 0 && local) fq[slot] = (t << 13) | (i << 11) | (row << 4) | nib;
-                        bool queued = local;
-                        if (nib && !local) {
-                            uint32_t g = 0;
-                            if ((lane & 3u) == 0) {
-                                g = atomicAdd(&P.status->n_fix, 1u);
-                                if (g < P.fix_cap)
-                                    P.fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | s;
-                            }
-                            g = __shfl_sync(0xffffffffu, g, lane & ~3u);
-                            queued = g < P.fix_cap;
-                        }
-                        float out = live ? est : 0.f;
-                        if (need && !queued) out = exact_likelihood(d, P.V, P.T, b, t, s);
+                        bool here = false;
+                        const float out = enqueue(need, t, i, s, b, live ? est : 0.f, here);
+                        if (here && P.lazy) note_exact(out, t, i, s);
                         if (valid) P.L[(uint64_t)t * d.N + s] = out;
+                    }
+                }
+            }
+            if (P.lazy) {
+                // pass 2: contenders for each window's maximum (upper bound reaching the
+                // window's largest lower bound) are recomputed; the other certainly
+                // positive samples keep their estimate and get their inexact bit
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                for (uint32_t i = 0; i < P.ntiles; ++i) {
+                    const uint32_t s = t_s0[i] + row;
+                    const bool valid = row < t_rows[i];
+                    const bool live = valid && (uint64_t)s + d.W < d.N;
+                    const uint32_t wslot = valid ? i * kWinSlots + (s / d.W - t_w0[i]) : 0u;
+                    const float mlb = __int_as_float(s_mlb[wslot]);
+                    const uint32_t mv = __ballot_sync(0xffffffffu, valid);
+                    const uint32_t s_lane0 = t_s0[i] + qd * 32;
+                    for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
+                        float v[16];
+                        tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const uint32_t t = cg * 16 + e;
+                            if (t >= d.M) continue;
+                            const float b = sbias[t];
+                            const float est = v[e] + b;
+                            const float bd = bnd[i * d.M + t];
+                            const bool certain = live && est - bd > 0.f;
+                            const bool contender = certain && est + bd >= mlb;
+                            bool here = false;
+                            const float out = enqueue(contender, t, i, s, b, est, here);
+                            if (here) {
+                                note_exact(out, t, i, s);
+                                P.L[(uint64_t)t * d.N + s] = out;
+                            }
+                            const uint32_t mi = __ballot_sync(0xffffffffu, certain && !contender);
+                            if (lane == 0 && mv) {
+                                uint32_t* wd = P.inexact + (uint64_t)t * P.nwb + (s_lane0 >> 5);
+                                const uint32_t off = s_lane0 & 31u;
+                                atomicAnd(wd, ~(mv << off));
+                                if (mi) atomicOr(wd, mi << off);
+                                if (off && (mv >> (32 - off))) {
+                                    atomicAnd(wd + 1, ~(mv >> (32 - off)));
+                                    if (mi >> (32 - off)) atomicOr(wd + 1, mi >> (32 - off));
+                                }
+                            }
+                        }
                     }
                 }
             }
@@ -382,11 +479,11 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
     // landing in distinct banks.
     const uint32_t nq = min(*nfq, kFixCap);
     if (threadIdx.x == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
-    if (nq == 0) return;
+    if (nq == 0 && !P.lazy) return;
     // the strips were written by bulk copies and read by the MMAs (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     const uint32_t Cp = P.Cq * 4;
-    {
+    if (nq > 0) {
         // each 4-channel block of R8 16-byte rows becomes 4 channel rows of R8
         // floats in the same bytes: one block at a time, read fully, then written
         constexpr uint32_t kPer = 2;   // R8 <= 256 rows <= kPer * blockDim
@@ -448,6 +545,33 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         if (mask & 2u) Lr[1] = a1;
         if (mask & 4u) Lr[2] = a2;
         if (mask & 8u) Lr[3] = a3;
+        if (P.lazy) {
+            const float a[4] = {a0, a1, a2, a3};
+#pragma unroll
+            for (uint32_t k = 0; k < 4; ++k) {
+                if (!((mask >> k) & 1u) || !(a[k] > 0.f)) continue;
+                const uint32_t sk = t_s0[i] + r0 + k, w = sk / W, slot = i * kWinSlots + (w - t_w0[i]);
+                atomicMax(&s_key[slot], window_key(a[k], t, sk - w * W));
+                s_pos[slot] = 1u;
+            }
+        }
+    }
+    if (!P.lazy) return;
+    // publish each touched window's maximum key and positive flag: a listed window
+    // belongs to this CTA alone (stored); a tile of the whole-chunk pass shares its
+    // edge windows with the neighbouring tiles (combined with atomics on zeroed arrays)
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < P.ntiles * kWinSlots; e += blockDim.x) {
+        const uint32_t i = e / kWinSlots, j = e - i * kWinSlots;
+        if (t_rows[i] == 0 || j > (t_s0[i] + t_rows[i] - 1) / W - t_w0[i]) continue;
+        const uint32_t w = t_w0[i] + j;
+        if (P.list != nullptr) {
+            P.wkey[w] = s_key[e];
+            P.wpos[w] = (uint8_t)(s_pos[e] ? 1 : 0);
+        } else {
+            if (s_key[e]) atomicMax(&P.wkey[w], s_key[e]);
+            if (s_pos[e]) P.wpos[w] = 1;
+        }
     }
 }
 
@@ -456,10 +580,21 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
 // set.  A thread carries the four samples' sequential sums side by side: per 4
 // taps one 16-byte template load and 4 voltage loads feed 16 multiply-adds
 // (each sum still adds its products one at a time, in the reference's order).
+// With lazy exactness, each positive exact value also enters its window's key
+// and positive flag (after the likelihood kernel has published the CTA's own).
+__device__ __forceinline__ void note_window(const Dims& d, unsigned long long* wkey, uint8_t* wpos, float v,
+                                            uint32_t t, uint32_t s)
+{
+    if (wkey == nullptr || !(v > 0.f)) return;
+    const uint32_t w = s / d.W;
+    atomicMax(&wkey[w], window_key(v, t, s - w * d.W));
+    wpos[w] = 1;
+}
+
 __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
                              const float* __restrict__ Tp, const float* __restrict__ bias,
                              const unsigned long long* __restrict__ fix, uint32_t cap, const DevStatus* status,
-                             float* L)
+                             float* L, unsigned long long* wkey, uint8_t* wpos)
 {
     const uint32_t n = min(status->n_fix, cap);
     const uint32_t W = d.W, Wp = (W + 3) & ~3u, W4 = W & ~3u;
@@ -469,7 +604,11 @@ __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* _
         const float b = bias[t];
         if ((uint64_t)s0 + W + 3 > d.N) {   // the run reaches the end of the chunk: one sample at a time
             for (uint32_t k = 0; k < 4; ++k)
-                if ((mask >> k) & 1u) L[(uint64_t)t * d.N + s0 + k] = exact_likelihood(d, V, T, b, t, s0 + k);
+                if ((mask >> k) & 1u) {
+                    const float v = exact_likelihood(d, V, T, b, t, s0 + k);
+                    L[(uint64_t)t * d.N + s0 + k] = v;
+                    note_window(d, wkey, wpos, v, t, s0 + k);
+                }
             continue;
         }
         float a0 = b, a1 = b, a2 = b, a3 = b;
@@ -501,10 +640,82 @@ __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* _
             }
         }
         float* Lr = L + (uint64_t)t * d.N + s0;
-        if (mask & 1u) Lr[0] = a0;
-        if (mask & 2u) Lr[1] = a1;
-        if (mask & 4u) Lr[2] = a2;
-        if (mask & 8u) Lr[3] = a3;
+        if (mask & 1u) { Lr[0] = a0; note_window(d, wkey, wpos, a0, t, s0); }
+        if (mask & 2u) { Lr[1] = a1; note_window(d, wkey, wpos, a1, t, s0 + 1); }
+        if (mask & 4u) { Lr[2] = a2; note_window(d, wkey, wpos, a2, t, s0 + 2); }
+        if (mask & 8u) { Lr[3] = a3; note_window(d, wkey, wpos, a3, t, s0 + 3); }
+    }
+}
+
+// Per-window argmax from the window keys (compute_template_maximum_likelihood,
+// binary_pursuit.cl:350-441): the maximum over the 3-window span of listed window
+// id is the best of the maxima of windows id-1, id and id+1, compared by value,
+// then template, then sample (the span's first maximum in template-major order).
+// The flags and outputs are those of argmax_kernel.
+__global__ void argmax_lazy_kernel(Dims d, const uint32_t* __restrict__ list, uint32_t nlist,
+                                   const unsigned long long* __restrict__ wkey, const uint8_t* __restrict__ wpos,
+                                   float* best_lik, uint32_t* best_lab, uint32_t* best_idx, uint8_t* check,
+                                   uint8_t* orech, uint32_t* ov_idx, uint32_t* ov_lab)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nlist; k += gridDim.x * blockDim.x) {
+        const uint32_t id = list[k];
+        const uint64_t start = (uint64_t)id * d.W, end = start + d.W;
+        if (end >= (uint64_t)d.N - d.W) continue;
+        bool have = false;
+        float bv = 0.f;
+        uint32_t bt = 0, bs = 0;
+        const uint32_t x0 = id > 0 ? id - 1 : 0;
+        for (uint32_t x = x0; x <= id + 1; ++x) {   // id + 1 < nw: end + W < N
+            const unsigned long long key = wkey[x];
+            if (key == 0ull) continue;
+            const float v = __uint_as_float((uint32_t)(key >> 32));
+            const uint32_t code = 0xFFFFFFFFu - (uint32_t)key;
+            const uint32_t t = code >> 10, s = x * d.W + (code & 1023u);
+            if (!have || v > bv || (v == bv && (t < bt || (t == bt && s < bs)))) {
+                have = true; bv = v; bt = t; bs = s;
+            }
+        }
+        if (wpos[id]) check[id] = 1;
+        uint32_t lab = best_lab[id], idx = best_idx[id];
+        float bl = 0.f;
+        if (have) { bl = bv; lab = bt; idx = bs; }
+        orech[id] = (bl > 0.f && idx >= start && idx < end) ? 1 : 0;
+        best_lik[id] = bl;
+        best_lab[id] = lab;
+        best_idx[id] = idx;
+        ov_idx[id] = idx;
+        ov_lab[id] = lab;
+    }
+}
+
+// Before a pass's residual: likelihood estimates (inexact bit set) of windows
+// whose voltage the residual changes and which the next pass does not
+// recompute (check == 0 once the pass's flags are final) are replaced by their
+// exact values from the voltage they were computed on, so that every estimate
+// left in L can later be made exact from the current voltage.  One CTA per
+// spike of the pass; a spike at s changes the likelihood of samples (s-W, s+W).
+__global__ void lazy_fix_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
+                                const float* __restrict__ bias, const uint32_t* __restrict__ pidx,
+                                const DevStatus* status, const uint8_t* __restrict__ check, float* L,
+                                uint32_t* inexact, uint32_t nwb)
+{
+    const uint32_t n = status->n_spikes;
+    for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const uint64_t s = pidx[k];
+        const uint64_t lo = s + 1 >= d.W ? s + 1 - d.W : 0;
+        const uint64_t hi = s + d.W < d.N ? s + d.W : d.N;   // samples [lo, hi)
+        for (uint64_t x = lo / d.W; x * d.W < hi && x < d.nw; ++x) {
+            if (check[x] != 0) continue;   // relisted: recomputed next pass before any read
+            const uint64_t a = x * d.W, b = min((uint64_t)d.N, a + d.W);
+            for (uint64_t e = threadIdx.x; e < (uint64_t)d.M * (b - a); e += blockDim.x) {
+                const uint32_t t = (uint32_t)(e / (b - a));
+                const uint32_t q = (uint32_t)(a + e % (b - a));
+                uint32_t* wd = inexact + (uint64_t)t * nwb + (q >> 5);
+                if (!((*wd >> (q & 31u)) & 1u)) continue;
+                L[(uint64_t)t * d.N + q] = exact_likelihood(d, V, T, bias[t], t, q);
+                atomicAnd(wd, ~(1u << (q & 31u)));
+            }
+        }
     }
 }
 
@@ -605,7 +816,8 @@ bool tc_config(const Dims& d, TcConfig* c)
         c->stages = 3;
         while (c->group > 1 && strips + c->stages * c->group * (size_t)c->Np * 32 > 160 * 1024) c->group >>= 1;
         c->smem = strips + c->stages * (size_t)c->group * c->Np * 32 + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
-                  (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + (size_t)kFixCap * 4 + 4 + 1024;
+                  (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + (size_t)kFixCap * 4 + 4 +
+                  (size_t)c->ntiles * 4 + (size_t)c->ntiles * kWinSlots * 16 + 8 + 1024;
         // CTAs resident on one SM must not ask for more than its 512 TMEM columns
         // together (a blocked tcgen05.alloc would wait for another CTA to finish):
         // ask for enough shared memory that at most 512 / ncols of them fit
@@ -623,6 +835,31 @@ bool tc_supported(const Dims& d)
 {
     TcConfig c;
     return tc_config(d, &c);
+}
+
+int launch_argmax_lazy(const Dims& d, const Work& w, const uint32_t* list, uint32_t nlist, cudaStream_t st)
+{
+    if (nlist == 0) return FBP_OK;
+    const Layout& L = *w.lay;
+    count_launch();
+    const uint32_t grid = std::min<uint32_t>((nlist + 255) / 256, 148 * 16);
+    argmax_lazy_kernel<<<grid, 256, 0, st>>>(d, list, nlist, w.at<unsigned long long>(L.off_wkey),
+                                             w.at<uint8_t>(L.off_wpos), w.best_lik(), w.best_lab(), w.best_idx(),
+                                             w.check(), w.orech(), w.ov_idx(), w.ov_lab());
+    FBP_CUDA(cudaGetLastError());
+    return FBP_OK;
+}
+
+int launch_lazy_fix(const Dims& d, const Work& w, const float* V, const float* T, const float* bias,
+                    uint32_t nmax, cudaStream_t st)
+{
+    if (nmax == 0) return FBP_OK;
+    const Layout& L = *w.lay;
+    count_launch();
+    lazy_fix_kernel<<<std::min<uint32_t>(nmax, 148 * 16), 256, 0, st>>>(
+        d, V, T, bias, w.pidx(), w.status(), w.check(), w.L(), w.at<uint32_t>(L.off_inexact), (uint32_t)L.nwb);
+    FBP_CUDA(cudaGetLastError());
+    return FBP_OK;
 }
 
 int launch_tc_prepare_templates(const Dims& d, const Work& w, const float* T, cudaStream_t st)
@@ -656,10 +893,9 @@ int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const
 }
 
 int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T, const float* bias,
-                         const uint32_t* list, uint32_t nlist, float* Lk, bool refresh_voltage, cudaStream_t st,
+                         const uint32_t* list, uint32_t nlist, float* Lk, bool lazy, cudaStream_t st,
                          uint64_t* n_fix_out)
 {
-    (void)refresh_voltage;
     (void)n_fix_out;
     if (nlist == 0) return FBP_OK;
     TcConfig c;
@@ -696,6 +932,15 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     const double u24 = 1.0 / 16777216.0;
     P.k_a = (float)(1.1 * (1.0 / 512.0 + (2.0 * n + 8.0) * 4.0 * u24 + (n + 2.0) * u24));
     P.k_b = (float)(1.1 * (n + 8.0) * 4.0 * u24);
+    P.lazy = lazy ? 1u : 0u;
+    P.wkey = lazy ? w.at<unsigned long long>(L.off_wkey) : nullptr;
+    P.wpos = lazy ? w.at<uint8_t>(L.off_wpos) : nullptr;
+    P.inexact = lazy ? w.at<uint32_t>(L.off_inexact) : nullptr;
+    P.nwb = (uint32_t)L.nwb;
+    if (lazy && all) {
+        FBP_CUDA(cudaMemsetAsync(P.wkey, 0, (size_t)d.nw * 8, st));
+        FBP_CUDA(cudaMemsetAsync(P.wpos, 0, (size_t)d.nw, st));
+    }
     FBP_CUDA(cudaMemsetAsync(&w.status()->n_fix, 0, 4, st));
     FBP_CUDA(cudaFuncSetAttribute(lik_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
     const uint32_t grid = (uint32_t)((items + c.ntiles - 1) / c.ntiles);
@@ -705,7 +950,7 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
         lik_tc_kernel<<<grid, kThreads, c.smem, st>>>(P);
     }
     KScope ks(&fbp_chunk_stats::ms_fixup, st);
-    fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, P.Tp, bias, P.fix, P.fix_cap, w.status(), Lk);
+    fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, P.Tp, bias, P.fix, P.fix_cap, w.status(), Lk, P.wkey, P.wpos);
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }

@@ -241,6 +241,7 @@ __global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
     const uint32_t nflag = status->n_flag;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint32_t wi = lane >> 2, bs = lane & 3;
+    unsigned long long macs = 0;   // multiply-adds this thread does
     for (uint32_t base = blockIdx.x * kPcWin; base < kc; base += gridDim.x * kPcWin) {
         __syncthreads();
         if (threadIdx.x < kPcWin) {
@@ -281,6 +282,7 @@ __global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
 #pragma unroll
                 for (int r = 0; r < kPcR; ++r) acc[q][r] = 0.f;
             const int vb = (int)b0 - gm.o;
+            if (jhi > jlo) macs += (unsigned long long)Q * kPcR * (uint32_t)(jhi - jlo) * Cu;
             for (uint32_t ci = 0; ci < Cu; ++ci) {
                 const float* vr = vw + (size_t)ci * gm.SLc;
                 const float* tr = Ts + (size_t)ci * Wp;
@@ -315,6 +317,9 @@ __global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
             }
         }
     }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) macs += __shfl_xor_sync(0xffffffffu, macs, off);
+    if (lane == 0 && macs) atomicAdd(&const_cast<DevStatus*>(status)->pc_macs, macs);
 }
 
 // Exact pair likelihood in the reference's float order (binary_pursuit.cl:578-632),

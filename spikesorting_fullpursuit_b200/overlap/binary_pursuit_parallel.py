@@ -29,7 +29,10 @@ Differences, all documented:
 * Keyword-only extras: ``mode`` ("fast": tensor-core likelihood and screened
   overlap recheck, both exact; "plain": scalar FP32 kernels), ``device``,
   ``work_group_size`` (the reference's kernel work-group size, 256, whose
-  execution order the results follow), ``max_passes``, ``verbose``,
+  execution order the results follow), ``max_passes``,
+  ``dedupe_chunk_seams`` (drop a chunk's spikes that the previous chunk found
+  with the same index and label in their 3-window overlap; off by default,
+  where the output is the reference's, duplicates included), ``verbose``,
   ``return_stats``.
 """
 from __future__ import annotations
@@ -81,6 +84,30 @@ def plan_chunks(n_samples, n_chans, n_templates, template_samples_per_chan, samp
         onsets.append(onset)
         onset += chunk - 3 * W
     return onsets, chunk
+
+
+def seam_duplicates(prev_idx, prev_lab, idx, lab, seam_start):
+    """Which of a chunk's spikes the previous chunk already found.
+
+    Chunks overlap by 3 windows (binary_pursuit_parallel.py:498-507) and the
+    reference keeps the spikes both chunks find in the overlap
+    (binary_pursuit_parallel.py:1491, left to later post-processing).  A spike of
+    this chunk at or after ``seam_start`` (the chunk's onset) is a duplicate when
+    the previous chunk has a spike with the same index and label.  Indices are
+    absolute sample indices; returns a boolean mask over ``idx``."""
+    idx = np.asarray(idx, dtype=np.int64)
+    lab = np.asarray(lab, dtype=np.int64)
+    prev_idx = np.asarray(prev_idx, dtype=np.int64)
+    prev_lab = np.asarray(prev_lab, dtype=np.int64)
+    dup = np.zeros(idx.size, dtype=bool)
+    if idx.size == 0 or prev_idx.size == 0:
+        return dup
+    sel = prev_idx >= seam_start
+    width = int(max(lab.max(initial=0), prev_lab.max(initial=0))) + 1
+    prev_keys = np.unique(prev_idx[sel] * width + prev_lab[sel])
+    mine = idx >= seam_start
+    dup[mine] = np.isin(idx[mine] * width + lab[mine], prev_keys, assume_unique=False)
+    return dup
 
 
 def _ptr(t):
@@ -215,8 +242,8 @@ class _Pursuer:
 
 def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
                    kernels_path=None, max_gpu_memory=None, *, mode="fast", device=None,
-                   work_group_size=WORK_GROUP_SIZE, max_passes=MAX_PASSES, verbose=True,
-                   return_stats=False):
+                   work_group_size=WORK_GROUP_SIZE, max_passes=MAX_PASSES,
+                   dedupe_chunk_seams=False, verbose=True, return_stats=False):
     """Find template spikes in ``voltage`` by binary pursuit on the GPU.
 
     See the module docstring for the contract; the arguments mean what they
@@ -265,10 +292,18 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
             si, sl, clips = pursuer.chunk(voltage[:, start:stop], get_clips)
             if si.size == 0:
                 continue
-            idx_all.append(si.astype(np.int64) + start)
+            ab = si.astype(np.int64) + start
+            if dedupe_chunk_seams and idx_all:
+                keep = ~seam_duplicates(idx_all[-1], lab_all[-1], ab, sl, start)
+                ab, sl = ab[keep], sl[keep]
+                if get_clips and len(clips):
+                    clips = clips[keep]
+                if ab.size == 0:
+                    continue
+            idx_all.append(ab)
             lab_all.append(sl)
             clips_all.append(clips)
-            bool_all.append(np.ones(si.size, dtype=bool))
+            bool_all.append(np.ones(ab.size, dtype=bool))
     finally:
         if pursuer is not None:
             pursuer.close()

@@ -16,7 +16,8 @@ def pytest_configure(config):
 
 
 def golden_names():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    """Pursuit goldens (tests/golden/*.npz other than the post-processing ones)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("postprocess_"))
 
 
 _VOLTAGE_CACHE = {}
@@ -60,6 +61,28 @@ def load_golden(name):
         "empty": bool(d["empty_result"]),
     }
     return _golden_voltage(d, meta), si, sm, call, expect, meta
+
+
+# Goldens whose CPU checks take minutes: in the default CPU run the oracle is
+# checked end to end on two of them only; FBP_FULL_GOLDEN=1 runs every check on
+# all of them (the chunk internals, the reference kernels' restated host loop,
+# the 3 s slice of the 10-minute recording, which is regenerated, and the
+# 200-template case, whose brute-force oracle takes minutes).
+HEAVY_GOLDENS = {"linear16_bench_1s": "end_to_end", "tetrode_cfg0_30s": "end_to_end",
+                 "linear16_bench_3s": "full_only", "dense64_m200_0p1s": "full_only"}
+
+
+def full_golden_run():
+    return os.environ.get("FBP_FULL_GOLDEN", "") not in ("", "0")
+
+
+def skip_heavy(name, check):
+    """Skip a CPU check of a heavy golden unless the full run is requested."""
+    mode = HEAVY_GOLDENS.get(name)
+    if mode is None or full_golden_run():
+        return
+    if mode == "full_only" or check != "end_to_end":
+        pytest.skip("heavy golden: set FBP_FULL_GOLDEN=1 for this check")
 
 
 @pytest.fixture(params=golden_names())

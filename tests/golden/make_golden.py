@@ -71,6 +71,9 @@ CASES = {
     # the benchmark's own recording (16 ch, 40 templates, 10 min), its leading second
     "linear16_bench_1s": (dict(config="linear16", seed=1, slice_s=1.0),
                           dict(n_max_shift_inds=100), dict(clips=True, store_voltage=True)),
+    # the same recording's leading 3 seconds (voltage regenerated, not stored)
+    "linear16_bench_3s": (dict(config="linear16", seed=1, slice_s=3.0),
+                          dict(n_max_shift_inds=100), dict(clips=False, store_voltage=False)),
     # the tetrode configuration in full: 4 ch, 30 s, 6 templates
     "tetrode_cfg0_30s": (dict(config="tetrode", seed=1),
                          dict(n_max_shift_inds=100), dict(clips=False, store_voltage=False)),
@@ -79,7 +82,7 @@ CASES = {
                           dict(n_max_shift_inds=75), dict(clips=True, store_voltage=True)),
 }
 
-HEAVY = ("linear16_bench_1s", "tetrode_cfg0_30s", "dense64_m200_0p1s")
+HEAVY = ("linear16_bench_1s", "linear16_bench_3s", "tetrode_cfg0_30s", "dense64_m200_0p1s")
 
 
 def make_inputs(rec_kw):

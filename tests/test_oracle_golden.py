@@ -4,7 +4,10 @@ import hashlib
 
 import numpy as np
 
+import pytest
+
 import oracle
+from conftest import golden_names, load_golden, skip_heavy
 
 
 def _sha(a):
@@ -15,8 +18,10 @@ def _same(got, want):
     return np.array_equal(np.asarray(got), np.asarray(want))
 
 
-def test_oracle_matches_reference_outputs(golden):
-    name, V, si, sm, call, expect, meta = golden
+@pytest.mark.parametrize("name", golden_names())
+def test_oracle_matches_reference_outputs(name):
+    skip_heavy(name, "end_to_end")
+    V, si, sm, call, expect, meta = load_golden(name)
     out = oracle.binary_pursuit(V, np.float32, si, copy.deepcopy(sm),
                                 global_mem_size=meta["global_mem_size"],
                                 work_group_size=meta["work_group_size"], **call)
@@ -34,9 +39,11 @@ def test_oracle_matches_reference_outputs(golden):
         assert np.asarray(clips).size == 0
 
 
-def test_oracle_chunk_internals(golden):
+@pytest.mark.parametrize("name", golden_names())
+def test_oracle_chunk_internals(name):
     """First-pass likelihood buffer, final residual and per-pass spike counts."""
-    name, V, si, sm, call, expect, meta = golden
+    skip_heavy(name, "internals")
+    V, si, sm, call, expect, meta = load_golden(name)
     W = si["n_samples_per_chan"]
     S = call.get("n_max_shift_inds")
     if S is None:
@@ -64,14 +71,15 @@ def test_oracle_chunk_internals(golden):
             assert _sha(resid) == ch["resid_sha256"], name
 
 
-def test_reference_kernels_with_restated_host_loop(golden):
+@pytest.mark.parametrize("name", golden_names())
+def test_reference_kernels_with_restated_host_loop(name):
     """oracle/ref_host.py (the CPU baseline of bench.py) reproduces the goldens."""
     import os
-    import pytest
     if not os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libbp_ref.so")):
         pytest.skip("oracle/_ref not built")
     import ref_host
-    name, V, si, sm, call, expect, meta = golden
+    skip_heavy(name, "reference_kernels")
+    V, si, sm, call, expect, meta = load_golden(name)
     ev, lab = ref_host.binary_pursuit(V, si, copy.deepcopy(sm), global_mem_size=meta["global_mem_size"],
                                       work_group_size=meta["work_group_size"], **call)
     if expect["empty"]:
