@@ -197,6 +197,24 @@ int fbp_adjoint_grad(const fbp_dims* dims, const float* voltage, const float* te
                      const float* shift, uint32_t n_spikes, double scale, double* grad_templates64,
                      float* grad_templates, float* grad_amplitude, float* grad_shift, void* stream);
 
+/* ---- noise model of the thresholds (pre-pursuit) ---- */
+
+/* compute_separability_metrics + set_bp_threshold
+ * (spikesorting_fullpursuit/overlap/neuron_separability.py:113-195, 319-331) per
+ * template, on the device: template_SS (np.sum(T**2) in the templates' type,
+ * numpy's pairwise order), the FP64 likelihood variance sum_c T_c' Cov_c T_c,
+ * lower_CI = 0.5 SS - sigma_bp_ci sqrt(var), the threshold -0.5 SS +
+ * sigma_bp_noise sqrt(var) (then max(threshold, 0, lower_CI) when
+ * apply_bp_threshold), the contamination norm.sf(threshold, -0.5 SS, sqrt(var))
+ * and the peak channel argmax|T| / W.  templates [M][C][W] float32 or float64
+ * (templates_f64), channel_cov float64 [C][W][W]; template_ss has the templates'
+ * type; other outputs float64 [M], peak_channel int64 [M]. */
+int fbp_separability(const void* templates, int templates_f64, const double* channel_cov,
+                     uint32_t n_templates, uint32_t n_chans, uint32_t template_len, double sigma_bp_noise,
+                     double sigma_bp_ci, int apply_bp_threshold, void* template_ss, double* variance,
+                     double* lower_ci, double* threshold, double* contamination, int64_t* peak_channel,
+                     void* stream);
+
 /* ---- post-pursuit duplicate removal (device-resident output) ---- */
 
 /* Mean clip of one unit, np.mean(clips, axis=0) in float32 (rows summed in

@@ -27,7 +27,7 @@ FBP_TIMING = 0x4
 EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_pursue_chunk",
            "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc",
            "fbp_adjoint_loss", "fbp_adjoint_grad", "fbp_mean_clip", "fbp_bp_duplicates_workspace",
-           "fbp_bp_duplicates")
+           "fbp_bp_duplicates", "fbp_separability")
 NOALLOC_MAX_SPIKES = 65536
 PASS_RING = 64
 ABI_VERSION = 3
@@ -109,6 +109,9 @@ def lib():
     L.fbp_bp_duplicates_workspace.restype = sz
     L.fbp_bp_duplicates.argtypes = [vp, vp, vp, vp, u32, u32, ctypes.c_int64, vp, vp, sz, vp]
     L.fbp_bp_duplicates.restype = ctypes.c_int
+    dbl, i32 = ctypes.c_double, ctypes.c_int
+    L.fbp_separability.argtypes = [vp, i32, vp, u32, u32, u32, dbl, dbl, i32, vp, vp, vp, vp, vp, vp, vp]
+    L.fbp_separability.restype = ctypes.c_int
     _lib = L
     return L
 

@@ -16,8 +16,9 @@ def pytest_configure(config):
 
 
 def golden_names():
-    """Pursuit goldens (tests/golden/*.npz other than the post-processing ones)."""
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("postprocess_"))
+    """Pursuit goldens (tests/golden/*.npz other than those of the pre- and post-processing steps)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN)
+                  if f.endswith(".npz") and not f.startswith(("postprocess_", "separability_")))
 
 
 _VOLTAGE_CACHE = {}
