@@ -60,7 +60,11 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--config", default="linear16", choices=["linear16", "tetrode", "dense64"])
+    p.add_argument("--config", default="linear16", choices=["linear16", "tetrode", "dense64", "batched"])
+    p.add_argument("--batch-streams", type=int, default=8,
+                   help="batched: segments pursued at once (one CUDA stream and host thread each)")
+    p.add_argument("--batch-scale", type=float, default=1.0,
+                   help="batched: segment durations times this factor (1.0: uniform 5-60 s)")
     p.add_argument("--duration", type=float, default=None, help="seconds of recording (default: config's)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -195,6 +199,9 @@ def main():
         return
     if args.adjoint:
         run_adjoint(args)
+        return
+    if args.config == "batched":
+        run_batched(args)
         return
     import torch
     import torch.distributed as dist
@@ -457,6 +464,116 @@ def run_adjoint(args):
         "config": {"workload": "adjoint: %d ch x %d samples (%.0f s at %d Hz), %d templates x %d samples, %d spikes "
                                "(from one pursuit), linear-interpolation shifts" % (C, N, N / si["sampling_rate"],
                                                                                    si["sampling_rate"], M, W, n)}}))
+
+
+def run_batched(args):
+    """Many independent segments (64, uniform 5-60 s at 40 kHz, 4-12 channels,
+    5-30 templates each): one after another on one stream, against
+    --batch-streams of them at once, each on a CUDA stream of its own issued by
+    its own host thread (longest segments first).  A step is one pursuit of all
+    segments; both schedules must give identical spikes per segment."""
+    import queue
+    import threading
+
+    import torch
+    from spikesorting_fullpursuit_b200 import _native, synth
+
+    dev = torch.device("cuda", 0)
+    segs = synth.batched_segments(2, scale=args.batch_scale)
+    lib = _native.lib()
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    flags = _native.FBP_OVERLAP_RECHECK
+    jobs = []
+    for V, si, sm in segs:
+        C, N = V.shape
+        W = si["n_samples_per_chan"]
+        T = np.float32(sm["templates"])
+        M = T.shape[0]
+        d = _native.dims(C, N, M, W, W - 1)
+        cap = 8 * (N // W + 1) + 1024
+        jobs.append({
+            "d": d, "V0": torch.from_numpy(V).to(dev), "V": torch.empty((C, N), device=dev),
+            "T": torch.from_numpy(T).to(dev), "b": torch.from_numpy(np.float32(-0.5 * sm["template_SS"])).to(dev),
+            "th": torch.from_numpy(np.float32(sm["neuron_lower_thresholds"])).to(dev),
+            "ws": torch.empty(_native.workspace_bytes(d, flags), dtype=torch.uint8, device=dev),
+            "idx": torch.empty(cap, dtype=torch.int32, device=dev), "lab": torch.empty(cap, dtype=torch.int32, device=dev),
+            "cap": cap, "units": C * N, "seconds": N / si["sampling_rate"]})
+    order = sorted(range(len(jobs)), key=lambda k: -jobs[k]["units"])
+
+    def pursue(j, stream):
+        n = ctypes.c_uint32(0)
+        _native.check(lib.fbp_pursue_chunk(ctypes.byref(j["d"]), flags, P(j["V"]), P(j["T"]), P(j["b"]), P(j["th"]),
+                                           P(j["ws"]), j["ws"].numel(), P(j["idx"]), P(j["lab"]), j["cap"],
+                                           ctypes.byref(n), None, 0, ctypes.c_void_p(stream.cuda_stream)))
+        j["n"] = n.value
+
+    def step(nstreams):
+        for j in jobs:
+            j["V"].copy_(j["V0"])
+        torch.cuda.synchronize()
+        main = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        if nstreams <= 1:
+            for k in order:
+                pursue(jobs[k], main)
+        else:
+            streams = [torch.cuda.Stream(dev) for _ in range(nstreams)]
+            todo = queue.Queue()
+            for k in order:
+                todo.put(k)
+            errors = []
+
+            def worker(st):
+                st.wait_event(e0)
+                while True:
+                    try:
+                        k = todo.get_nowait()
+                    except queue.Empty:
+                        return
+                    try:
+                        pursue(jobs[k], st)
+                    except BaseException as exc:  # re-raised below
+                        errors.append(exc)
+            threads = [threading.Thread(target=worker, args=(st,)) for st in streams]
+            for t in threads:
+                t.start()
+            for t in threads:
+                t.join()
+            if errors:
+                raise errors[0]
+            for st in streams:
+                main.wait_stream(st)
+        e1.record(main)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), [(j["idx"][:j["n"]].cpu().numpy().copy(), j["lab"][:j["n"]].cpu().numpy().copy())
+                                     for j in jobs]
+
+    res = {}
+    for mode, ns in (("sequential", 1), ("concurrent", args.batch_streams)):
+        for _ in range(args.warmup):
+            step(ns)
+        ms, out = [], None
+        for _ in range(args.steps):
+            t, out = step(ns)
+            ms.append(t)
+        res[mode] = (float(np.sum(ms)), out)
+    same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+               for a, b in zip(res["sequential"][1], res["concurrent"][1]))
+    units = sum(j["units"] for j in jobs) * args.steps
+    v_seq = units / (res["sequential"][0] * 1e-3) / 1e6
+    v_con = units / (res["concurrent"][0] * 1e-3) / 1e6
+    print(json.dumps({
+        "metric": METRIC + " (batched segments)", "value": v_con, "unit": "Msample*ch/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["concurrent"][0] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched: %d segments, %.0f s in total (uniform %.1f-%.1f s), 4-12 channels, 5-30 "
+                               "templates, 40 kHz" % (len(jobs), sum(j["seconds"] for j in jobs),
+                                                     5 * args.batch_scale, 60 * args.batch_scale),
+                   "streams": args.batch_streams},
+        "sequential": {"value": v_seq, "ms_per_step": res["sequential"][0] / args.steps},
+        "speedup_vs_sequential": v_con / v_seq, "identical_spikes": bool(same),
+        "spikes": int(sum(o[0].size for o in res["concurrent"][1]))}), flush=True)
 
 
 def cpu_baseline(args, Vfull, sifull, sm):

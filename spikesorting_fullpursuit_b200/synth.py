@@ -233,9 +233,100 @@ CONFIGS = {
 }
 
 
+def make_recording_gpu(seed, device, n_chans, fs, duration_s, n_units, layout="index", pitch_um=50.0, nbhd=None,
+                       sigma_um=60.0, rate_model=("uniform", 5.0, 30.0), overlap_frac=0.0,
+                       clip_width=(-1.0e-3, 1.5e-3), amp=(6.0, 12.0), n_cov_clips=10000):
+    """make_recording for recordings too long to filter on the host: the same
+    templates, spike trains and threshold model (numpy, seeded), with the noise
+    drawn and band-passed on the GPU: white N(0, 1) per channel (torch
+    generator seeded from ``seed``), the zero-phase magnitude |H(f)|^2 of the
+    same 4th-order Butterworth band-pass applied in the frequency domain
+    (what forward-backward filtering does away from the edges), rescaled to
+    unit standard deviation; spikes added with index_add on the device.
+    Returns the voltage as a tensor [C, N] float32 on ``device``, sort_info,
+    metrics."""
+    import torch
+    from scipy import signal
+
+    rng = np.random.default_rng(seed)
+    n_samples = int(round(duration_s * fs))
+    clip_width = list(clip_width)
+    templates, W, pre = make_templates(rng, n_units, n_chans, fs, clip_width, layout, pitch_um, nbhd, sigma_um, amp)
+    if rate_model[0] == "uniform":
+        rates = rng.uniform(rate_model[1], rate_model[2], size=n_units)
+    else:
+        rates = np.minimum(np.exp(rng.normal(np.log(rate_model[1]), 0.6, size=n_units)), rate_model[2])
+    hi = min(8000.0, 0.45 * fs)
+    sos = signal.butter(4, [300.0, hi], btype="band", fs=fs, output="sos")
+    freqs = np.fft.rfftfreq(n_samples, d=1.0 / fs)
+    _, h = signal.sosfreqz(sos, worN=freqs, fs=fs)
+    gain = torch.from_numpy((np.abs(h) ** 2).astype(np.float32)).to(device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed))
+    V = torch.empty((n_chans, n_samples), dtype=torch.float32, device=device)
+    for c in range(n_chans):
+        x = torch.randn(n_samples, generator=gen, device=device, dtype=torch.float32)
+        y = torch.fft.irfft(torch.fft.rfft(x) * gain, n=n_samples)
+        V[c] = y / y.std()
+        del x, y
+    noise_head = V[:, :min(n_samples, int(fs * 10))].cpu().numpy()
+    covs = noise_covariance(rng, noise_head, W, n_cov_clips)
+    times, labels = spike_trains(rng, n_units, duration_s, fs, rates, overlap_frac=overlap_frac)
+    scales = rng.normal(1.0, 0.1, size=times.size)
+    onset = times - pre
+    ok = (onset >= 0) & (onset + W <= n_samples)
+    onset, lab, sc = onset[ok], labels[ok], scales[ok]
+    T3 = torch.from_numpy(templates.reshape(n_units, n_chans, W)).to(device)
+    taps = torch.arange(W, device=device)
+    on = torch.from_numpy(onset).to(device)
+    lb = torch.from_numpy(lab).to(device)
+    scd = torch.from_numpy(sc.astype(np.float32)).to(device)
+    for c in range(n_chans):
+        units_on = torch.nonzero(torch.any(T3[:, c, :] != 0, dim=1)).flatten()
+        sel = torch.isin(lb, units_on)
+        if not bool(sel.any()):
+            continue
+        cols = (on[sel][:, None] + taps[None, :]).reshape(-1)
+        vals = (scd[sel][:, None] * T3[lb[sel], c, :]).reshape(-1)
+        V[c].index_add_(0, cols, vals)
+    sort_info = {
+        "sampling_rate": fs, "clip_width": clip_width, "n_samples_per_chan": W, "n_channels": n_chans,
+        "n_samples": n_samples, "do_overlap_recheck": True, "get_adjusted_clips": False,
+        "sigma_bp_noise": 3.719, "sigma_bp_CI": None,
+    }
+    return V, sort_info, separability_metrics(templates, covs, n_chans, W)
+
+
+def batched_segments(seed, n_segments=64, min_s=5.0, max_s=60.0, chans=(4, 12), units=(5, 30), fs=40000,
+                     scale=1.0):
+    """Independent segments of uneven length (uniform in [min_s, max_s] seconds,
+    times ``scale``), each with its own channel count and templates, generated as
+    the tetrode configuration with lognormal rates: a list of
+    (voltage, sort_info, separability_metrics)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_segments):
+        dur = float(rng.uniform(min_s, max_s)) * scale
+        C = int(rng.integers(chans[0], chans[1] + 1))
+        M = int(rng.integers(units[0], units[1] + 1))
+        V, si, sm, _ = make_recording(int(rng.integers(1 << 31)), n_chans=C, fs=fs, duration_s=dur, n_units=M,
+                                      layout="index", rate_model=("lognormal", 10.0, 80.0))
+        out.append((V, si, sm))
+    return out
+
+
 def config_recording(name, seed, duration_s=None, **overrides):
     kw = dict(CONFIGS[name])
     if duration_s is not None:
         kw["duration_s"] = duration_s
     kw.update(overrides)
     return make_recording(seed, **kw)
+
+
+def config_recording_gpu(name, seed, device, duration_s=None, **overrides):
+    """config_recording with the noise generated on the GPU (make_recording_gpu)."""
+    kw = dict(CONFIGS[name])
+    if duration_s is not None:
+        kw["duration_s"] = duration_s
+    kw.update(overrides)
+    return make_recording_gpu(seed, device, **kw)
