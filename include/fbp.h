@@ -197,6 +197,32 @@ int fbp_adjoint_grad(const fbp_dims* dims, const float* voltage, const float* te
                      const float* shift, uint32_t n_spikes, double scale, double* grad_templates64,
                      float* grad_templates, float* grad_amplitude, float* grad_shift, void* stream);
 
+/* ---- the pursuit's templates and noise covariances (pre-pursuit) ---- */
+
+/* Clips of n spikes on the listed channels (get_clips,
+ * spikesorting_fullpursuit/processing/clip_utils.py:501-632, for indices whose
+ * window lies inside the voltage): clips[k][i*win_len + j] =
+ * voltage[chans[i]][event_indices[k] + win0 + j].  voltage float32 [n_chans][n_samples],
+ * clips float32 [n][n_nbr*win_len]. */
+int fbp_gather_clips(const float* voltage, uint32_t n_chans, uint64_t n_samples, const uint32_t* chans,
+                     uint32_t n_nbr, const int64_t* event_indices, uint32_t n, int32_t win0,
+                     uint32_t win_len, float* clips, void* stream);
+
+/* Robust template of n clips (calculate_robust_template, clip_utils.py:202-248):
+ * per clip sample, in float32, the median of the values within one MAD/0.6745 of
+ * the median (strictly), else the median; medians as np.median. */
+int fbp_robust_template(const float* clips, uint32_t n, uint32_t clip_len, float* tmpl, void* stream);
+
+/* Per-channel noise covariances of clip-minus-template residuals
+ * (get_channel_covariance_matrix, spikesorting_fullpursuit/overlap/full_binary_pursuit.py:863-923):
+ * residual row r = clips[r] - templates[unit_of[r]] (float32); for each channel c,
+ * over the rows listed in rows[c][0..n_rows) (int64 [n_chans][n_rows]: the
+ * reference draws them per channel), cov[c] (float64 [W][W], W =
+ * n_samples_per_chan) is np.cov of samples [c*W, (c+1)*W) with ddof 0. */
+int fbp_residual_covariance(const float* clips, const float* templates, const uint32_t* unit_of,
+                            const int64_t* rows, uint32_t n_rows, uint32_t clip_len, uint32_t n_chans,
+                            uint32_t n_samples_per_chan, double* cov, void* stream);
+
 /* ---- noise model of the thresholds (pre-pursuit) ---- */
 
 /* compute_separability_metrics + set_bp_threshold

@@ -18,7 +18,7 @@ def pytest_configure(config):
 def golden_names():
     """Pursuit goldens (tests/golden/*.npz other than those of the pre- and post-processing steps)."""
     return sorted(f[:-4] for f in os.listdir(GOLDEN)
-                  if f.endswith(".npz") and not f.startswith(("postprocess_", "separability_")))
+                  if f.endswith(".npz") and not f.startswith(("postprocess_", "separability_", "preprocess_")))
 
 
 _VOLTAGE_CACHE = {}
