@@ -115,10 +115,9 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
         if (cap > (32ull << 20)) cap = 32ull << 20;
         L->n_fix_cap = cap + 4096;
         L->off_fix = take(L->n_fix_cap * 8);
-        L->nwb = (N + 31) / 32 + 1;
         L->off_wkey = take(nw * 8);
         L->off_wpos = take(nw);
-        L->off_inexact = take(M * L->nwb * 4);
+        L->off_wflag = take(nw * M);
     }
     if (!(flags & FBP_PLAIN_FP32) && (flags & FBP_OVERLAP_RECHECK)) {
         const uint64_t xt = M * M * S2 * S2 * 4;
@@ -246,7 +245,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         FBP_TRY(launch_tc_prepare_templates(d, w, templates, st));
         FBP_TRY(launch_tc_update_voltage(d, w, voltage, nullptr, nullptr, 0, true, st));
     }
-    if (lazy) FBP_CUDA(cudaMemsetAsync(w.base + lay.off_inexact, 0, lay.M * lay.nwb * 4, st));
+    if (lazy) FBP_CUDA(cudaMemsetAsync(w.base + lay.off_wflag, 0, lay.nw * lay.M, st));
     if (!plain && overlap) FBP_TRY(launch_overlap_tables(d, w, templates, st));
     uint32_t nlist = d.nw, total = 0;
     api_detail::StageTimer tm;

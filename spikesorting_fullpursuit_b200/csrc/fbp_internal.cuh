@@ -79,9 +79,8 @@ struct Layout {
     size_t off_vt_hi, off_tt_hi, off_tpad, off_fix, off_tnorm;
     uint64_t Cp, Mp, n_fix_cap, vq_rows;
     // lazy exactness of the tensor-core likelihood: per-window maximum keys and
-    // positive flags, one "estimate" bit per likelihood sample ([M][nwb] words)
-    size_t off_wkey, off_wpos, off_inexact;
-    uint64_t nwb;
+    // positive flags, and per (window, template) "row holds estimates" flags
+    size_t off_wkey, off_wpos, off_wflag;
     // screened overlap recheck: truncated energies Et[M][S2] (f64), pair cross
     // terms XT[M][M][S2][S2] (f32), partial correlations G[gbatch][M][S2] (f32),
     // template processing order perm[M]
@@ -123,10 +122,9 @@ struct Work {
 };
 
 // Where the tensor-core likelihood left estimates (lazy exactness): readers of
-// a likelihood value recompute it exactly when its bit is set.
+// a positive likelihood value recompute it exactly when its window row is flagged.
 struct LazyRef {
-    const uint32_t* inexact;   // [M][nwb] bits, or null: L is exact wherever read
-    uint32_t nwb;
+    const uint8_t* wflag;      // [nw][M] flags, or null: L is exact wherever read
     const float* V;
     const float* T;
     const float* bias;

@@ -494,14 +494,15 @@ __device__ float exact_lik(const Dims& d, const float* __restrict__ V, const flo
     return acc;
 }
 
-// L[t][s], made exact where the tensor-core likelihood left an estimate (its
-// voltage is unchanged since, so the current voltage gives the exact value).
+// L[t][s], made exact where the tensor-core likelihood may have left an estimate
+// (a positive value in a flagged window row; the window's voltage is unchanged
+// since it was computed, so the current voltage gives the exact value).
 __device__ __forceinline__ float lik_value(const Dims& d, const float* __restrict__ L, const LazyRef& z, uint32_t t,
                                            uint32_t s)
 {
-    if (z.inexact != nullptr && ((z.inexact[(uint64_t)t * z.nwb + (s >> 5)] >> (s & 31u)) & 1u))
-        return exact_lik(d, z.V, z.T, z.bias[t], t, s);
-    return L[(uint64_t)t * d.N + s];
+    const float v = L[(uint64_t)t * d.N + s];
+    if (z.wflag != nullptr && v > 0.f && z.wflag[(uint64_t)(s / d.W) * d.M + t]) return exact_lik(d, z.V, z.T, z.bias[t], t, s);
+    return v;
 }
 
 __global__ void parse_kernel(Dims d, const float* __restrict__ L, const float* __restrict__ theta,
@@ -960,10 +961,9 @@ int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint
 {
     if (nflag_max == 0) return FBP_OK;
     const uint32_t g = grid_for(nflag_max, 256);
-    LazyRef z{nullptr, 0, V, T, bias};
+    LazyRef z{nullptr, V, T, bias};
     if (lazy) {
-        z.inexact = w.at<uint32_t>(w.lay->off_inexact);
-        z.nwb = (uint32_t)w.lay->nwb;
+        z.wflag = w.at<uint8_t>(w.lay->off_wflag);
     }
     count_launch(5);
     parse_kernel<<<g, 256, 0, st>>>(d, w.L(), theta, w.flag(), w.status(), w.keys(), w.best_lik(),

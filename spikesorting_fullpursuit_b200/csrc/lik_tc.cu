@@ -43,7 +43,8 @@ constexpr int kTile = 128;         // samples per UMMA tile (M)
 constexpr int kThreads = 192;
 constexpr uint64_t kWaitNs = 250ull * 1000ull * 1000ull;   // longest mbarrier wait (global timer)
 constexpr uint32_t kFixCap = 1024;   // runs recomputed in the CTA itself; more go to the global queue
-constexpr uint32_t kWinSlots = 130;  // windows one 128-sample tile can touch (W >= 1)
+// windows one tile of 128 consecutive samples can touch
+__host__ __device__ __forceinline__ uint32_t win_slots(uint32_t W) { return (kTile + W - 1) / W + 1; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -164,12 +165,12 @@ struct TcParams {
     float k_a, k_b;       // bound = k_a * sum_c |T_tc| |V_c strip| + k_b * |bias_t|
     // lazy exactness (pursuit): only samples whose sign is uncertain and the
     // contenders for each window's maximum are recomputed exactly; every other
-    // positive sample keeps its estimate and its bit in `inexact` is set
+    // positive sample keeps its estimate and its (window, template) row is flagged
     uint32_t lazy;
     unsigned long long* wkey;   // [nw] window maximum: see window_key()
     uint8_t* wpos;              // [nw] 1 if the window holds a positive likelihood
-    uint32_t* inexact;          // [M][nwb] one bit per sample: L holds an estimate
-    uint32_t nwb;               // 32-bit words per template row of `inexact`
+    uint8_t* wflag;             // [nw][M] 1: the window's row of template t holds estimates
+    uint32_t wslots;            // win_slots(W): window slots per tile in shared memory
 };
 
 // Key of a positive likelihood v at (template t, sample s) of window w:
@@ -219,10 +220,11 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
     uint32_t* fq = reinterpret_cast<uint32_t*>(sbias + d.M);      // [kFixCap] runs: t | tile | row | mask
     uint32_t* nfq = fq + kFixCap;
     uint32_t* t_w0 = nfq + 1;                                      // [ntiles] first window of each tile
-    int* s_mlb = reinterpret_cast<int*>(t_w0 + P.ntiles);          // [ntiles][kWinSlots] max lower bound (float bits)
-    uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_mlb + P.ntiles * kWinSlots);   // [ntiles][kWinSlots]
+    int* s_mlb = reinterpret_cast<int*>(t_w0 + P.ntiles);          // [ntiles][wslots] max lower bound (float bits)
+    uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_mlb + P.ntiles * P.wslots);   // [ntiles][wslots]
     unsigned long long* s_key = reinterpret_cast<unsigned long long*>(
-        (reinterpret_cast<uintptr_t>(s_pos + P.ntiles * kWinSlots) + 7) & ~(uintptr_t)7);   // [ntiles][kWinSlots]
+        (reinterpret_cast<uintptr_t>(s_pos + P.ntiles * P.wslots) + 7) & ~(uintptr_t)7);   // [ntiles][wslots]
+    uint8_t* s_inex = reinterpret_cast<uint8_t*>(s_key + P.ntiles * P.wslots);   // [ntiles][wslots][M]
 
     const uint32_t ksteps = d.W * (P.Cq / 2);
     const uint32_t ngroups = (ksteps + P.group - 1) / P.group;
@@ -252,11 +254,13 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         t_rows[i] = rows;
         t_w0[i] = s0 / d.W;
     }
-    for (uint32_t e = threadIdx.x; e < P.ntiles * kWinSlots; e += blockDim.x) {
+    for (uint32_t e = threadIdx.x; e < P.ntiles * P.wslots; e += blockDim.x) {
         s_mlb[e] = 0;
         s_pos[e] = 0;
         s_key[e] = 0ull;
     }
+    if (P.lazy)
+        for (uint32_t e = threadIdx.x; e < P.ntiles * P.wslots * d.M; e += blockDim.x) s_inex[e] = 0;
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(P.ncols));
@@ -380,7 +384,7 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
             // exact positive value v at (t, s) of tile i: window maximum and sign
             auto note_exact = [&](float v, uint32_t t, uint32_t i, uint32_t s) {
                 if (!(v > 0.f)) return;
-                const uint32_t w = s / d.W, slot = i * kWinSlots + (w - t_w0[i]);
+                const uint32_t w = s / d.W, slot = i * P.wslots + (w - t_w0[i]);
                 atomicMax(&s_key[slot], window_key(v, t, s - w * d.W));
                 s_pos[slot] = 1u;
             };
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
                 const uint32_t s = t_s0[i] + row;
                 const bool valid = row < t_rows[i];
                 const bool live = valid && (uint64_t)s + d.W < d.N;
-                const uint32_t wslot = valid ? i * kWinSlots + (s / d.W - t_w0[i]) : 0u;
+                const uint32_t wslot = valid ? i * P.wslots + (s / d.W - t_w0[i]) : 0u;
                 for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
                     float v[16];
                     tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
@@ -417,16 +421,14 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
             if (P.lazy) {
                 // pass 2: contenders for each window's maximum (upper bound reaching the
                 // window's largest lower bound) are recomputed; the other certainly
-                // positive samples keep their estimate and get their inexact bit
+                // positive samples keep their estimate, and their window row is flagged
                 asm volatile("bar.sync 1, 128;" ::: "memory");
                 for (uint32_t i = 0; i < P.ntiles; ++i) {
                     const uint32_t s = t_s0[i] + row;
                     const bool valid = row < t_rows[i];
                     const bool live = valid && (uint64_t)s + d.W < d.N;
-                    const uint32_t wslot = valid ? i * kWinSlots + (s / d.W - t_w0[i]) : 0u;
+                    const uint32_t wslot = valid ? i * P.wslots + (s / d.W - t_w0[i]) : 0u;
                     const float mlb = __int_as_float(s_mlb[wslot]);
-                    const uint32_t mv = __ballot_sync(0xffffffffu, valid);
-                    const uint32_t s_lane0 = t_s0[i] + qd * 32;
                     for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
                         float v[16];
                         tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
@@ -445,17 +447,7 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
                                 note_exact(out, t, i, s);
                                 P.L[(uint64_t)t * d.N + s] = out;
                             }
-                            const uint32_t mi = __ballot_sync(0xffffffffu, certain && !contender);
-                            if (lane == 0 && mv) {
-                                uint32_t* wd = P.inexact + (uint64_t)t * P.nwb + (s_lane0 >> 5);
-                                const uint32_t off = s_lane0 & 31u;
-                                atomicAnd(wd, ~(mv << off));
-                                if (mi) atomicOr(wd, mi << off);
-                                if (off && (mv >> (32 - off))) {
-                                    atomicAnd(wd + 1, ~(mv >> (32 - off)));
-                                    if (mi >> (32 - off)) atomicOr(wd + 1, mi >> (32 - off));
-                                }
-                            }
+                            if (certain && !contender) s_inex[wslot * d.M + t] = 1;
                         }
                     }
                 }
@@ -550,7 +542,7 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
 #pragma unroll
             for (uint32_t k = 0; k < 4; ++k) {
                 if (!((mask >> k) & 1u) || !(a[k] > 0.f)) continue;
-                const uint32_t sk = t_s0[i] + r0 + k, w = sk / W, slot = i * kWinSlots + (w - t_w0[i]);
+                const uint32_t sk = t_s0[i] + r0 + k, w = sk / W, slot = i * P.wslots + (w - t_w0[i]);
                 atomicMax(&s_key[slot], window_key(a[k], t, sk - w * W));
                 s_pos[slot] = 1u;
             }
@@ -561,8 +553,8 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
     // belongs to this CTA alone (stored); a tile of the whole-chunk pass shares its
     // edge windows with the neighbouring tiles (combined with atomics on zeroed arrays)
     __syncthreads();
-    for (uint32_t e = threadIdx.x; e < P.ntiles * kWinSlots; e += blockDim.x) {
-        const uint32_t i = e / kWinSlots, j = e - i * kWinSlots;
+    for (uint32_t e = threadIdx.x; e < P.ntiles * P.wslots; e += blockDim.x) {
+        const uint32_t i = e / P.wslots, j = e - i * P.wslots;
         if (t_rows[i] == 0 || j > (t_s0[i] + t_rows[i] - 1) / W - t_w0[i]) continue;
         const uint32_t w = t_w0[i] + j;
         if (P.list != nullptr) {
@@ -572,6 +564,15 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
             if (s_key[e]) atomicMax(&P.wkey[w], s_key[e]);
             if (s_pos[e]) P.wpos[w] = 1;
         }
+    }
+    // estimate flags of the windows' template rows: a listed window's are all
+    // written; the whole-chunk pass sets them on zeroed flags
+    for (uint32_t e = threadIdx.x; e < P.ntiles * P.wslots * d.M; e += blockDim.x) {
+        const uint32_t slot = e / d.M, t = e - slot * d.M;
+        const uint32_t i = slot / P.wslots, j = slot - i * P.wslots;
+        if (t_rows[i] == 0 || j > (t_s0[i] + t_rows[i] - 1) / W - t_w0[i]) continue;
+        const uint8_t f = s_inex[e];
+        if (P.list != nullptr || f) P.wflag[(uint64_t)(t_w0[i] + j) * d.M + t] = f;
     }
 }
 
@@ -688,16 +689,17 @@ __global__ void argmax_lazy_kernel(Dims d, const uint32_t* __restrict__ list, ui
     }
 }
 
-// Before a pass's residual: likelihood estimates (inexact bit set) of windows
-// whose voltage the residual changes and which the next pass does not
-// recompute (check == 0 once the pass's flags are final) are replaced by their
-// exact values from the voltage they were computed on, so that every estimate
-// left in L can later be made exact from the current voltage.  One CTA per
+// Before a pass's residual: the positive values of flagged (window, template)
+// rows -- rows that may hold estimates -- of windows whose voltage the residual
+// changes and which the next pass does not recompute (check == 0 once the pass's
+// flags are final) are replaced by their exact values from the voltage they were
+// computed on, and the flags cleared, so that every estimate left in L can later
+// be made exact from the current voltage.  One CTA per
 // spike of the pass; a spike at s changes the likelihood of samples (s-W, s+W).
 __global__ void lazy_fix_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
                                 const float* __restrict__ bias, const uint32_t* __restrict__ pidx,
                                 const DevStatus* status, const uint8_t* __restrict__ check, float* L,
-                                uint32_t* inexact, uint32_t nwb)
+                                uint8_t* wflag)
 {
     const uint32_t n = status->n_spikes;
     for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
@@ -707,14 +709,17 @@ __global__ void lazy_fix_kernel(Dims d, const float* __restrict__ V, const float
         for (uint64_t x = lo / d.W; x * d.W < hi && x < d.nw; ++x) {
             if (check[x] != 0) continue;   // relisted: recomputed next pass before any read
             const uint64_t a = x * d.W, b = min((uint64_t)d.N, a + d.W);
+            // positive values of flagged rows may be estimates: make them exact (the
+            // others are certainly <= 0 and are read for their sign only)
             for (uint64_t e = threadIdx.x; e < (uint64_t)d.M * (b - a); e += blockDim.x) {
                 const uint32_t t = (uint32_t)(e / (b - a));
                 const uint32_t q = (uint32_t)(a + e % (b - a));
-                uint32_t* wd = inexact + (uint64_t)t * nwb + (q >> 5);
-                if (!((*wd >> (q & 31u)) & 1u)) continue;
-                L[(uint64_t)t * d.N + q] = exact_likelihood(d, V, T, bias[t], t, q);
-                atomicAnd(wd, ~(1u << (q & 31u)));
+                if (!wflag[x * d.M + t]) continue;
+                float* lp = L + (uint64_t)t * d.N + q;
+                if (*lp > 0.f) *lp = exact_likelihood(d, V, T, bias[t], t, q);
             }
+            __syncthreads();
+            for (uint32_t t = threadIdx.x; t < d.M; t += blockDim.x) wflag[x * d.M + t] = 0;
         }
     }
 }
@@ -795,33 +800,38 @@ bool tc_config(const Dims& d, TcConfig* c)
     const uint32_t Cp = (d.C + 7) / 8 * 8;
     c->Cq = Cp / 4;
     c->Np = (d.M + 15) / 16 * 16;
-    // up to 128 template columns (two tiles take at most 256 TMEM columns, so two or
-    // more CTAs share an SM); larger template sets use the exact FP32 likelihood kernel
-    if (c->Np > 128) return false;
+    // one MMA (cta_group::1, M = 128) takes at most 256 template columns
+    if (c->Np > 256) return false;
     c->R8 = (kTile + d.W - 1 + 7) / 8 * 8;
-    // two tiles per CTA: up to 48 template columns four CTAs fit an SM (TMEM <= 128
-    // columns and about 54 KB of shared memory each), so one CTA's epilogue and exact
-    // recomputations overlap the others' MMAs (measured faster than four tiles in two
-    // CTAs, or one tile); wider template sets fit fewer CTAs (see the TMEM rule below)
-    c->ntiles = 512 / c->Np;
-    if (c->ntiles > 2) c->ntiles = 2;
-    if (c->ntiles == 0) return false;
+    // two tiles per CTA up to 128 template columns: up to 64 columns four CTAs fit an
+    // SM (TMEM <= 128 columns and about 54 KB of shared memory each), so one CTA's
+    // epilogue overlaps the others' MMAs (measured faster than four tiles in two CTAs,
+    // or one tile); above 128 columns one tile per CTA and two CTAs per SM
+    c->ntiles = c->Np <= 128 ? 2 : 1;
     for (;;) {
         const uint32_t cols = c->ntiles * c->Np;
         c->ncols = 32;
         while (c->ncols < cols) c->ncols <<= 1;
-        const size_t strips = (size_t)c->ntiles * c->Cq * c->R8 * 16;
-        // template stages of about 6 KB (whole k-steps), three in the ring
-        c->group = (uint32_t)std::max<size_t>(1, (6 * 1024) / ((size_t)c->Np * 32));
-        c->stages = 3;
-        while (c->group > 1 && strips + c->stages * c->group * (size_t)c->Np * 32 > 160 * 1024) c->group >>= 1;
-        c->smem = strips + c->stages * (size_t)c->group * c->Np * 32 + (2 + 2 * c->stages) * 8 + 8 + c->ntiles * 8 +
-                  (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 + (size_t)kFixCap * 4 + 4 +
-                  (size_t)c->ntiles * 4 + (size_t)c->ntiles * kWinSlots * 16 + 8 + 1024;
         // CTAs resident on one SM must not ask for more than its 512 TMEM columns
-        // together (a blocked tcgen05.alloc would wait for another CTA to finish):
-        // ask for enough shared memory that at most 512 / ncols of them fit
-        const uint32_t fit = 512 / c->ncols;   // 1..4 (at most 4 by the launch bounds)
+        // together (a blocked tcgen05.alloc would wait for another CTA to finish)
+        const uint32_t fit = std::min<uint32_t>(4, 512 / c->ncols);
+        const size_t strips = (size_t)c->ntiles * c->Cq * c->R8 * 16;
+        const size_t kstep = (size_t)c->Np * 32;
+        // template stages of about 6 KB (whole k-steps), three in the ring
+        c->group = (uint32_t)std::max<size_t>(1, (6 * 1024) / kstep);
+        c->stages = 3;
+        while (c->group > 1 && strips + c->stages * c->group * kstep > 160 * 1024) c->group >>= 1;
+        const size_t misc = 8 + c->ntiles * 8 + (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 +
+                            (size_t)kFixCap * 4 + 4 + (size_t)c->ntiles * 4 + (size_t)c->ntiles * win_slots(d.W) * (16 + d.M) + 8 +
+                            1024;
+        auto total = [&](uint32_t stages) { return strips + stages * c->group * kstep + (2 + 2 * stages) * 8 + misc; };
+        if (fit < 4) {
+            // fewer CTAs share the SM: a deeper ring keeps more template bytes in flight
+            const size_t budget = (228 * 1024) / fit - 2 * 1024;
+            while (c->stages < 8 && total(c->stages + 1) <= budget) ++c->stages;
+        }
+        c->smem = total(c->stages);
+        // ask for enough shared memory that at most `fit` CTAs are resident on an SM
         if (fit < 4) c->smem = std::max<size_t>(c->smem, (228 * 1024) / (fit + 1) + 1024);
         if (c->smem <= 200 * 1024) return true;
         if (c->ntiles == 1) return false;
@@ -857,7 +867,7 @@ int launch_lazy_fix(const Dims& d, const Work& w, const float* V, const float* T
     const Layout& L = *w.lay;
     count_launch();
     lazy_fix_kernel<<<std::min<uint32_t>(nmax, 148 * 16), 256, 0, st>>>(
-        d, V, T, bias, w.pidx(), w.status(), w.check(), w.L(), w.at<uint32_t>(L.off_inexact), (uint32_t)L.nwb);
+        d, V, T, bias, w.pidx(), w.status(), w.check(), w.L(), w.at<uint8_t>(L.off_wflag));
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }
@@ -935,11 +945,12 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     P.lazy = lazy ? 1u : 0u;
     P.wkey = lazy ? w.at<unsigned long long>(L.off_wkey) : nullptr;
     P.wpos = lazy ? w.at<uint8_t>(L.off_wpos) : nullptr;
-    P.inexact = lazy ? w.at<uint32_t>(L.off_inexact) : nullptr;
-    P.nwb = (uint32_t)L.nwb;
+    P.wflag = lazy ? w.at<uint8_t>(L.off_wflag) : nullptr;
+    P.wslots = win_slots(d.W);
     if (lazy && all) {
         FBP_CUDA(cudaMemsetAsync(P.wkey, 0, (size_t)d.nw * 8, st));
         FBP_CUDA(cudaMemsetAsync(P.wpos, 0, (size_t)d.nw, st));
+        FBP_CUDA(cudaMemsetAsync(P.wflag, 0, (size_t)d.nw * d.M, st));
     }
     FBP_CUDA(cudaMemsetAsync(&w.status()->n_fix, 0, 4, st));
     FBP_CUDA(cudaFuncSetAttribute(lik_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));

@@ -254,7 +254,8 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     if not torch.cuda.is_available():
         raise RuntimeError("No GPU available")
     _native.lib()
-    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dev = (device if isinstance(device, torch.device)
+           else torch.device("cuda", torch.cuda.current_device() if device is None else int(device)))
     n_chans = int(voltage.shape[0])
     n_samples = int(voltage.shape[1])
     sampling_rate = sort_info["sampling_rate"]

@@ -57,7 +57,8 @@ def get_channel_covariance_matrix(clip_template_residuals, n_channels, n_samples
 
     if not torch.cuda.is_available():
         raise RuntimeError("No GPU available")
-    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dev = (device if isinstance(device, torch.device)
+           else torch.device("cuda", torch.cuda.current_device() if device is None else int(device)))
     R = np.vstack(clip_template_residuals)
     if R.dtype != np.float32:
         raise TypeError("residuals must be float32, got %s" % R.dtype)
@@ -79,7 +80,8 @@ def templates_and_covariances(clips_dict, voltage, all_chan_nbrs, spike_indices_
 
     if not torch.cuda.is_available():
         raise RuntimeError("No GPU available")
-    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dev = (device if isinstance(device, torch.device)
+           else torch.device("cuda", torch.cuda.current_device() if device is None else int(device)))
     Vd = voltage if isinstance(voltage, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(voltage, np.float32))
     Vd = Vd.to(dev)
     clips, templates, units = [], [], []

@@ -29,7 +29,8 @@ def _device_metrics(templates, channel_covariance_mats, n_chans, W, sigma_noise,
 
     if not torch.cuda.is_available():
         raise RuntimeError("No GPU available")
-    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dev = (device if isinstance(device, torch.device)
+           else torch.device("cuda", torch.cuda.current_device() if device is None else int(device)))
     T = np.ascontiguousarray(templates)
     f64 = T.dtype == np.float64
     if not f64 and T.dtype != np.float32:

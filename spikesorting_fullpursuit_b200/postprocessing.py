@@ -24,6 +24,13 @@ import numpy as np
 from . import _native
 
 
+def _device(torch, device):
+    """A CUDA torch.device from None (the current device), an index or a device."""
+    if isinstance(device, torch.device):
+        return device
+    return torch.device("cuda", torch.cuda.current_device() if device is None else int(device))
+
+
 def _dev_tensor(torch, x, dtype, dev):
     if isinstance(x, torch.Tensor):
         return x.to(device=dev, dtype=dtype).contiguous()
@@ -50,7 +57,7 @@ def remove_binary_pursuit_duplicates(event_indices, clips, unit_template, binary
     _check_float32(unit_template, "unit_template")
     if not torch.cuda.is_available():
         raise RuntimeError("No GPU available")
-    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dev = _device(torch, device)
     n = int(len(event_indices))
     if n == 0:
         return np.ones(0, dtype=bool)
@@ -74,7 +81,7 @@ def mean_clip(clips, device=None):
     import torch
 
     _check_float32(clips, "clips")
-    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dev = _device(torch, device)
     cl = _dev_tensor(torch, clips, torch.float32, dev)
     n = int(cl.shape[0])
     cl = cl.reshape(n, -1)
@@ -97,7 +104,7 @@ def remove_segment_duplicates(event_indices, neuron_labels, clips, binary_pursui
     ev = np.asarray(event_indices.cpu() if isinstance(event_indices, torch.Tensor) else event_indices)
     bp = np.asarray(binary_pursuit_bool.cpu() if isinstance(binary_pursuit_bool, torch.Tensor)
                     else binary_pursuit_bool)
-    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dev = _device(torch, device)
     cl = clips if isinstance(clips, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(clips))
     _check_float32(cl, "clips")
     cl = cl.to(dev)

@@ -27,7 +27,8 @@ def _torch_dev(device):
 
     if not torch.cuda.is_available():
         raise RuntimeError("No GPU available")
-    return torch, torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    return torch, (device if isinstance(device, torch.device)
+           else torch.device("cuda", torch.cuda.current_device() if device is None else int(device)))
 
 
 def _valid_range(event_indices, n_samples, window):
