@@ -65,6 +65,8 @@ def parse():
                    help="batched: segments pursued at once (one CUDA stream and host thread each)")
     p.add_argument("--batch-scale", type=float, default=1.0,
                    help="batched: segment durations times this factor (1.0: uniform 5-60 s)")
+    p.add_argument("--autotune", action="store_true",
+                   help="batched: launch shapes measured per segment shape (spikesorting_fullpursuit_b200.autotune)")
     p.add_argument("--duration", type=float, default=None, help="seconds of recording (default: config's)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -499,8 +501,19 @@ def run_batched(args):
             "idx": torch.empty(cap, dtype=torch.int32, device=dev), "lab": torch.empty(cap, dtype=torch.int32, device=dev),
             "cap": cap, "units": C * N, "seconds": N / si["sampling_rate"]})
     order = sorted(range(len(jobs)), key=lambda k: -jobs[k]["units"])
+    tune_s = 0.0
+    if args.autotune:
+        from spikesorting_fullpursuit_b200 import autotune
+        t0 = time.perf_counter()
+        for j, (V, si, sm) in zip(jobs, segs):
+            j["tuning"] = autotune.tune(j["V0"], np.float32(sm["templates"]), np.float32(-0.5 * sm["template_SS"]),
+                                        np.float32(sm["neuron_lower_thresholds"]), si["n_samples_per_chan"],
+                                        si["n_samples_per_chan"] - 1, device=dev)
+        tune_s = time.perf_counter() - t0
 
     def pursue(j, stream):
+        if args.autotune:
+            autotune.apply(j["tuning"])
         n = ctypes.c_uint32(0)
         _native.check(lib.fbp_pursue_chunk(ctypes.byref(j["d"]), flags, P(j["V"]), P(j["T"]), P(j["b"]), P(j["th"]),
                                            P(j["ws"]), j["ws"].numel(), P(j["idx"]), P(j["lab"]), j["cap"],
@@ -570,7 +583,9 @@ def run_batched(args):
         "config": {"workload": "batched: %d segments, %.0f s in total (uniform %.1f-%.1f s), 4-12 channels, 5-30 "
                                "templates, 40 kHz" % (len(jobs), sum(j["seconds"] for j in jobs),
                                                      5 * args.batch_scale, 60 * args.batch_scale),
-                   "streams": args.batch_streams},
+                   "streams": args.batch_streams,
+                   "autotune": {"on": bool(args.autotune), "tuning_s": tune_s,
+                                "shapes": len({json.dumps(j.get("tuning"), sort_keys=True) for j in jobs})}},
         "sequential": {"value": v_seq, "ms_per_step": res["sequential"][0] / args.steps},
         "speedup_vs_sequential": v_con / v_seq, "identical_spikes": bool(same),
         "spikes": int(sum(o[0].size for o in res["concurrent"][1]))}), flush=True)

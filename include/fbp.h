@@ -89,6 +89,21 @@ typedef struct fbp_chunk_stats {
  * (serialises the stream around each timed launch; for profiling). */
 #define FBP_TIMING 0x4u
 
+/* Launch shapes of the tensor-core likelihood and of the screened recheck's
+ * partial correlations; 0 leaves a choice to the library.  Values the sizes do
+ * not allow (shared memory, TMEM) fall back to the library's choice. */
+typedef struct fbp_tuning {
+    uint32_t lik_tiles;    /* 128-sample tiles per likelihood CTA: 1 or 2 */
+    uint32_t lik_group;    /* (tap, channel pair) steps of templates per staged copy */
+    uint32_t lik_stages;   /* staged template copies in flight: 2 to 8 */
+    uint32_t pc_group;     /* templates per partial-correlation CTA: 1, 2, 4 or 8 */
+} fbp_tuning;
+
+/* Set the calling thread's launch shapes for its later calls (NULL: the
+ * library's choices).  No counterpart in the reference (its work-group sizes are
+ * the device's preferred ones, binary_pursuit_parallel.py:577-582). */
+int fbp_set_tuning(const fbp_tuning* tuning);
+
 /* Library ABI version (FBP_ABI_VERSION). */
 int fbp_abi_version(void);
 

@@ -28,7 +28,7 @@ EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_purs
            "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc",
            "fbp_adjoint_loss", "fbp_adjoint_grad", "fbp_mean_clip", "fbp_bp_duplicates_workspace",
            "fbp_bp_duplicates", "fbp_separability", "fbp_gather_clips", "fbp_robust_template",
-           "fbp_residual_covariance")
+           "fbp_residual_covariance", "fbp_set_tuning")
 NOALLOC_MAX_SPIKES = 65536
 PASS_RING = 64
 ABI_VERSION = 3
@@ -62,6 +62,11 @@ class FbpChunkStats(ctypes.Structure):
         first = max(1, p - PASS_RING + 1)
         out["pass_spikes"] = [ring[(q - 1) % PASS_RING] for q in range(first, p + 1)]
         return out
+
+
+class FbpTuning(ctypes.Structure):
+    _fields_ = [("lik_tiles", ctypes.c_uint32), ("lik_group", ctypes.c_uint32), ("lik_stages", ctypes.c_uint32),
+                ("pc_group", ctypes.c_uint32)]
 
 
 class FbpError(RuntimeError):
@@ -119,6 +124,8 @@ def lib():
     L.fbp_robust_template.restype = ctypes.c_int
     L.fbp_residual_covariance.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, vp, vp]
     L.fbp_residual_covariance.restype = ctypes.c_int
+    L.fbp_set_tuning.argtypes = [P(FbpTuning)]
+    L.fbp_set_tuning.restype = ctypes.c_int
     _lib = L
     return L
 

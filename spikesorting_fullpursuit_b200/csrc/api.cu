@@ -27,6 +27,12 @@ int fail(int status, const std::string& msg)
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+fbp_tuning& tuning()
+{
+    static thread_local fbp_tuning t{};
+    return t;
+}
+
 KernelClock& kclock()
 {
     static thread_local KernelClock c;
@@ -185,6 +191,21 @@ using namespace fbp;
 extern "C" int fbp_abi_version(void) { return FBP_ABI_VERSION; }
 
 extern "C" const char* fbp_last_error(void) { return g_err.c_str(); }
+
+extern "C" int fbp_set_tuning(const fbp_tuning* t)
+{
+    g_err.clear();
+    if (t == nullptr) {
+        tuning() = fbp_tuning{};
+        return FBP_OK;
+    }
+    if (t->lik_tiles > 2 || (t->lik_stages != 0 && (t->lik_stages < 2 || t->lik_stages > 8)) ||
+        (t->pc_group != 0 && t->pc_group != 1 && t->pc_group != 2 && t->pc_group != 4 && t->pc_group != 8) ||
+        t->lik_group > 64)
+        return fail(FBP_E_ARG, "tuning value out of range");
+    tuning() = *t;
+    return FBP_OK;
+}
 
 extern "C" size_t fbp_workspace_bytes(const fbp_dims* dims, uint32_t flags)
 {

@@ -24,6 +24,9 @@ int fail(int status, const std::string& msg);
             return ::fbp::fail(FBP_E_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+// Launch shapes chosen by the caller (fbp_set_tuning), per thread; 0 = library choice.
+fbp_tuning& tuning();
+
 // ---------------------------------------------------------------------------
 // Per-call instrumentation: kernel launch counts, and (with FBP_TIMING) device
 // time per kernel family.  Thread-local; set up by the C-ABI entry points.

@@ -808,6 +808,8 @@ bool tc_config(const Dims& d, TcConfig* c)
     // epilogue overlaps the others' MMAs (measured faster than four tiles in two CTAs,
     // or one tile); above 128 columns one tile per CTA and two CTAs per SM
     c->ntiles = c->Np <= 128 ? 2 : 1;
+    const fbp_tuning& tu = tuning();
+    if (tu.lik_tiles == 1) c->ntiles = 1;
     for (;;) {
         const uint32_t cols = c->ntiles * c->Np;
         c->ncols = 32;
@@ -818,14 +820,14 @@ bool tc_config(const Dims& d, TcConfig* c)
         const size_t strips = (size_t)c->ntiles * c->Cq * c->R8 * 16;
         const size_t kstep = (size_t)c->Np * 32;
         // template stages of about 6 KB (whole k-steps), three in the ring
-        c->group = (uint32_t)std::max<size_t>(1, (6 * 1024) / kstep);
-        c->stages = 3;
+        c->group = tu.lik_group ? tu.lik_group : (uint32_t)std::max<size_t>(1, (6 * 1024) / kstep);
+        c->stages = tu.lik_stages ? tu.lik_stages : 3;
         while (c->group > 1 && strips + c->stages * c->group * kstep > 160 * 1024) c->group >>= 1;
         const size_t misc = 8 + c->ntiles * 8 + (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 +
                             (size_t)kFixCap * 4 + 4 + (size_t)c->ntiles * 4 + (size_t)c->ntiles * win_slots(d.W) * (16 + d.M) + 8 +
                             1024;
         auto total = [&](uint32_t stages) { return strips + stages * c->group * kstep + (2 + 2 * stages) * 8 + misc; };
-        if (fit < 4) {
+        if (fit < 4 && !tu.lik_stages) {
             // fewer CTAs share the SM: a deeper ring keeps more template bytes in flight
             const size_t budget = (228 * 1024) / fit - 2 * 1024;
             while (c->stages < 8 && total(c->stages + 1) <= budget) ++c->stages;

@@ -902,7 +902,9 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     // weighted by the measured cost per multiply-add of each group size (two
     // strip loads feed Q templates; below 4 the shared-memory loads dominate)
     double best = 0.0;
+    const int want_q = (int)tuning().pc_group;
     for (int Q = 8; Q >= 1; Q >>= 1) {
+        if (want_q && Q > want_q) continue;
         const double eff = Q >= 4 ? 1.0 : (Q == 2 ? 1.2 : 1.6);
         uint32_t cu_max = 0;
         double work = 0.0;
@@ -916,6 +918,11 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
         }
         const size_t smem = pc_smem_bytes(d, cu_max, Q);
         if (!(smem <= 110 * 1024 || (Q == 1 && smem <= 200 * 1024))) continue;
+        if (want_q) {   // the caller's group size, or the largest feasible one below it
+            pc.Q = Q;
+            pc.smem = smem;
+            break;
+        }
         if (pc.Q == 0 || work * eff < best) {
             pc.Q = Q;
             pc.smem = smem;

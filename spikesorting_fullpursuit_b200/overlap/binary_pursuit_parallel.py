@@ -32,7 +32,9 @@ Differences, all documented:
   execution order the results follow), ``max_passes``,
   ``dedupe_chunk_seams`` (drop a chunk's spikes that the previous chunk found
   with the same index and label in their 3-window overlap; off by default,
-  where the output is the reference's, duplicates included), ``verbose``,
+  where the output is the reference's, duplicates included), ``tuning``
+  (launch shapes: None for the library's, "auto" to measure them on the first
+  chunk with spikesorting_fullpursuit_b200.autotune, or a dict), ``verbose``,
   ``return_stats``.
 """
 from __future__ import annotations
@@ -42,7 +44,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
-from .. import _native
+from .. import _native, autotune
 from ..processing.conversions import time_window_to_samples
 
 WORK_GROUP_SIZE = 256
@@ -174,7 +176,7 @@ class _Pursuer:
     """Device buffers and the C-ABI calls for one binary_pursuit() call."""
 
     def __init__(self, torch, dev, n_chans, templates, bias, theta, W, S, max_chunk, flags,
-                 work_group_size, max_passes):
+                 work_group_size, max_passes, tuning=None):
         self.torch = torch
         self.dev = dev
         self.C, self.W, self.S = n_chans, W, S
@@ -192,6 +194,7 @@ class _Pursuer:
         self.ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
         self.V = torch.empty((n_chans, max_chunk), dtype=torch.float32, device=dev)
         self.up = _Uploader(torch, dev)
+        self.tuning = tuning
         self.stats = []
 
     def chunk(self, host_chunk, clips):
@@ -207,6 +210,19 @@ class _Pursuer:
         cap = min(4 * nw + 1024, most, 0xFFFFFFFF)
         stream = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
         L = _native.lib()
+        if self.tuning == "auto":
+            self.tuning = autotune.tune(V, self.T.cpu().numpy(), self.bias.cpu().numpy(), self.theta.cpu().numpy(),
+                                        self.W, self.S, overlap=bool(self.flags & _native.FBP_OVERLAP_RECHECK),
+                                        device=self.dev)
+        autotune.apply(self.tuning)
+        try:
+            return self._pursue(host_chunk, clips, V, d, N, nw, most, cap, stream, L)
+        finally:
+            autotune.apply(None)
+
+    def _pursue(self, host_chunk, clips, V, d, N, nw, most, cap, stream, L):
+        torch = self.torch
+        C = V.shape[0]
         for attempt in range(MAX_CAPACITY_RETRIES + 1):
             idx = torch.empty(cap, dtype=torch.int32, device=self.dev)
             lab = torch.empty(cap, dtype=torch.int32, device=self.dev)
@@ -243,7 +259,7 @@ class _Pursuer:
 def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
                    kernels_path=None, max_gpu_memory=None, *, mode="fast", device=None,
                    work_group_size=WORK_GROUP_SIZE, max_passes=MAX_PASSES,
-                   dedupe_chunk_seams=False, verbose=True, return_stats=False):
+                   dedupe_chunk_seams=False, tuning=None, verbose=True, return_stats=False):
     """Find template spikes in ``voltage`` by binary pursuit on the GPU.
 
     See the module docstring for the contract; the arguments mean what they
@@ -286,7 +302,7 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     if onsets:
         max_chunk = min(n_samples, chunk_len)
         pursuer = _Pursuer(torch, dev, n_chans, templates, bias, theta, W, S, max_chunk, flags,
-                           work_group_size, max_passes)
+                           work_group_size, max_passes, tuning)
     try:
         for start in onsets:
             stop = int(np.uint32(min(n_samples, start + chunk_len)))

@@ -124,3 +124,15 @@ def test_adjoint_arguments_fail_before_any_device_call(lib):
     assert lib.fbp_adjoint_loss(ctypes.byref(big), fake, fake, fake, fake, fake, fake, 1, loss,
                                 None) == _native.FBP_E_ARG
     assert b"tile" in lib.fbp_last_error()
+
+
+def test_tuning_validation(lib):
+    t = _native.FbpTuning(3, 0, 0, 0)   # more than two tiles per CTA
+    assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
+    t = _native.FbpTuning(0, 0, 9, 0)   # ring deeper than 8
+    assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
+    t = _native.FbpTuning(0, 0, 0, 3)   # group size not a power of two
+    assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
+    t = _native.FbpTuning(1, 2, 4, 4)
+    assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_OK
+    assert lib.fbp_set_tuning(None) == _native.FBP_OK
