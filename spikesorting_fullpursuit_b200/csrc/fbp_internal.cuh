@@ -24,6 +24,12 @@ int fail(int status, const std::string& msg);
             return ::fbp::fail(FBP_E_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+// Every launcher sets a kernel's dynamic shared-memory limit to this one value
+// (the opt-in maximum of a block on sm_100): the attribute belongs to the
+// kernel in the whole process, so calls on other threads that launched the same
+// kernel with other sizes never lower it under a launch in flight.
+constexpr int kMaxDynSmem = 227 * 1024;
+
 // Launch shapes chosen by the caller (fbp_set_tuning), per thread; 0 = library choice.
 fbp_tuning& tuning();
 
