@@ -502,48 +502,55 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
             __syncthreads();
         }
     }
-    const uint32_t W = d.W, W4 = W & ~3u, Wp = (W + 3) & ~3u;
+    const uint32_t W = d.W, Wp = (W + 3) & ~3u;
     const float* Vt = reinterpret_cast<const float*>(A);
-    for (uint32_t qi = threadIdx.x; qi < nq; qi += blockDim.x) {
+    // One warp per queued run.  Lanes 0..3 carry the run's four samples' sums, each
+    // adding its products one at a time in the reference order (channel-major, taps
+    // ascending); the warp loads each template channel row coalesced -- the next
+    // row while the current one is summed -- and broadcasts tap j by shuffle, so a
+    // run costs about one dependent add per tap rather than a global load per 4 taps.
+    const uint32_t nwarp = blockDim.x >> 5;
+    for (uint32_t qi = warp; qi < nq; qi += nwarp) {
         const uint32_t e = fq[qi];
         const uint32_t t = e >> 13, i = (e >> 11) & 3u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
-        float a0 = sbias[t], a1 = a0, a2 = a0, a3 = a0;
+        const uint32_t k = lane & 3u;   // lanes 4..31 repeat lanes 0..3 and are discarded
+        float acc = sbias[t];
+        const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
+        float tv[4], tn[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t x = lane + 32u * q;
+            tn[q] = x < W ? __ldg(tb + x) : 0.f;
+        }
         for (uint32_t c = 0; c < d.C; ++c) {
-            const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0;   // 16-byte aligned
-            const float* tr = P.Tp + ((uint64_t)t * d.C + c) * Wp;
-            uint32_t j = 0;
-            for (; j < W4; j += 4) {
-                const float4 t4 = __ldg(reinterpret_cast<const float4*>(tr + j));
-                const float4 lo = *reinterpret_cast<const float4*>(vr + j);
-                const float4 hi = *reinterpret_cast<const float4*>(vr + j + 4);
-                const float w0 = lo.x, w1 = lo.y, w2 = lo.z, w3 = lo.w, w4 = hi.x, w5 = hi.y, w6 = hi.z;
-                a0 = __fadd_rn(a0, __fmul_rn(t4.x, w0)); a1 = __fadd_rn(a1, __fmul_rn(t4.x, w1));
-                a2 = __fadd_rn(a2, __fmul_rn(t4.x, w2)); a3 = __fadd_rn(a3, __fmul_rn(t4.x, w3));
-                a0 = __fadd_rn(a0, __fmul_rn(t4.y, w1)); a1 = __fadd_rn(a1, __fmul_rn(t4.y, w2));
-                a2 = __fadd_rn(a2, __fmul_rn(t4.y, w3)); a3 = __fadd_rn(a3, __fmul_rn(t4.y, w4));
-                a0 = __fadd_rn(a0, __fmul_rn(t4.z, w2)); a1 = __fadd_rn(a1, __fmul_rn(t4.z, w3));
-                a2 = __fadd_rn(a2, __fmul_rn(t4.z, w4)); a3 = __fadd_rn(a3, __fmul_rn(t4.z, w5));
-                a0 = __fadd_rn(a0, __fmul_rn(t4.w, w3)); a1 = __fadd_rn(a1, __fmul_rn(t4.w, w4));
-                a2 = __fadd_rn(a2, __fmul_rn(t4.w, w5)); a3 = __fadd_rn(a3, __fmul_rn(t4.w, w6));
+#pragma unroll
+            for (int q = 0; q < 4; ++q) tv[q] = tn[q];
+            if (c + 1 < d.C) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t x = lane + 32u * q;
+                    tn[q] = x < W ? __ldg(tb + (uint64_t)(c + 1) * Wp + x) : 0.f;
+                }
             }
-            for (; j < W; ++j) {   // taps past the last multiple of 4
-                const float tv = __ldg(tr + j);
-                a0 = __fadd_rn(a0, __fmul_rn(tv, vr[j])); a1 = __fadd_rn(a1, __fmul_rn(tv, vr[j + 1]));
-                a2 = __fadd_rn(a2, __fmul_rn(tv, vr[j + 2])); a3 = __fadd_rn(a3, __fmul_rn(tv, vr[j + 3]));
+            const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0 + k;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+#pragma unroll
+                for (int jj = 0; jj < 32; ++jj) {
+                    const uint32_t j = 32u * q + jj;
+                    if (j < W) {   // the same for every lane
+                        const float tj = __shfl_sync(0xffffffffu, tv[q], jj);
+                        acc = __fadd_rn(acc, __fmul_rn(tj, vr[j]));
+                    }
+                }
             }
         }
-        float* Lr = P.L + (uint64_t)t * d.N + t_s0[i] + r0;
-        if (mask & 1u) Lr[0] = a0;
-        if (mask & 2u) Lr[1] = a1;
-        if (mask & 4u) Lr[2] = a2;
-        if (mask & 8u) Lr[3] = a3;
-        if (P.lazy) {
-            const float a[4] = {a0, a1, a2, a3};
-#pragma unroll
-            for (uint32_t k = 0; k < 4; ++k) {
-                if (!((mask >> k) & 1u) || !(a[k] > 0.f)) continue;
-                const uint32_t sk = t_s0[i] + r0 + k, w = sk / W, slot = i * P.wslots + (w - t_w0[i]);
-                atomicMax(&s_key[slot], window_key(a[k], t, sk - w * W));
+        if (lane < 4 && ((mask >> lane) & 1u)) {
+            const uint32_t sk = t_s0[i] + r0 + lane;
+            P.L[(uint64_t)t * d.N + sk] = acc;
+            if (P.lazy && acc > 0.f) {
+                const uint32_t w = sk / W, slot = i * P.wslots + (w - t_w0[i]);
+                atomicMax(&s_key[slot], window_key(acc, t, sk - w * W));
                 s_pos[slot] = 1u;
             }
         }
