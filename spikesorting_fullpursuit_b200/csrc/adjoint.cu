@@ -233,7 +233,7 @@ extern "C" int fbp_adjoint_loss(const fbp_dims* dims, const float* voltage, cons
     sumsq_kernel<<<148 * 4, 256, 0, st>>>(voltage, (uint64_t)A.C * A.N, loss);
     if (n_spikes) {
         const size_t smem = (size_t)A.C * (A.W + 2) * sizeof(double);
-        FBP_CUDA(cudaFuncSetAttribute(adjoint_loss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+        FBP_CUDA(allow_max_dyn_smem(adjoint_loss_kernel));
         count_launch();
         adjoint_loss_kernel<<<n_spikes < 148u * 16 ? n_spikes : 148u * 16, kAdjThreads, smem, st>>>(A, loss);
     }
@@ -257,7 +257,7 @@ extern "C" int fbp_adjoint_grad(const fbp_dims* dims, const float* voltage, cons
     FBP_CUDA(cudaMemsetAsync(grad_templates64, 0, nt * sizeof(double), st));
     if (n_spikes) {
         const size_t smem = (size_t)A.C * (A.W + 2) * sizeof(double);
-        FBP_CUDA(cudaFuncSetAttribute(adjoint_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+        FBP_CUDA(allow_max_dyn_smem(adjoint_grad_kernel));
         count_launch();
         adjoint_grad_kernel<<<n_spikes < 148u * 16 ? n_spikes : 148u * 16, kAdjThreads, smem, st>>>(
             A, scale, grad_templates64, grad_amplitude, grad_shift);

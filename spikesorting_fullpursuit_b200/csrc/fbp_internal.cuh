@@ -24,11 +24,22 @@ int fail(int status, const std::string& msg);
             return ::fbp::fail(FBP_E_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(e_)); \
     } while (0)
 
-// Every launcher sets a kernel's dynamic shared-memory limit to this one value
-// (the opt-in maximum of a block on sm_100): the attribute belongs to the
-// kernel in the whole process, so calls on other threads that launched the same
-// kernel with other sizes never lower it under a launch in flight.
-constexpr int kMaxDynSmem = 227 * 1024;
+// Every launcher sets a kernel's dynamic shared-memory limit to the largest the
+// device allows for that kernel (the block opt-in maximum less the kernel's
+// static shared memory): the attribute belongs to the kernel in the whole
+// process, and with one value per kernel, calls on other threads that launch the
+// same kernel with other sizes never lower it under a launch in flight.
+template <class Kernel>
+inline cudaError_t allow_max_dyn_smem(Kernel kernel)
+{
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+    if (e != cudaSuccess) return e;
+    int dev = 0, optin = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
+}
 
 // Launch shapes chosen by the caller (fbp_set_tuning), per thread; 0 = library choice.
 fbp_tuning& tuning();

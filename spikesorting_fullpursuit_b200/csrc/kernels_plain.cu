@@ -897,7 +897,7 @@ int launch_likelihood_exact(const Dims& d, const float* V, const float* T, const
     if (smem > budget) return fail(FBP_E_ARG, "channels x template_len too large for the likelihood kernel");
 #define FBP_LIK(QQ)                                                                               \
     case QQ:                                                                                      \
-        FBP_CUDA(cudaFuncSetAttribute(lik_exact_kernel<QQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem)); \
+        FBP_CUDA(allow_max_dyn_smem(lik_exact_kernel<QQ>)); \
         lik_exact_kernel<QQ><<<grid, threads, smem, st>>>(d, V, T, bias, list, nlist, L);       \
         break;
     count_launch();
@@ -943,7 +943,7 @@ int launch_overlap_plain(const Dims& d, const Work& w, const float* V, const flo
     smem = (smem + 15) & ~(size_t)15;
     smem += (size_t)kOvRound * 4 + 16;
     if (smem > 220 * 1024) return fail(FBP_E_ARG, "overlap recheck working set exceeds shared memory");
-    FBP_CUDA(cudaFuncSetAttribute(overlap_plain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    FBP_CUDA(allow_max_dyn_smem(overlap_plain_kernel));
     FBP_CUDA(cudaMemsetAsync(w.keys(), 0, sizeof(unsigned long long) * nflag_max, st));
     const uint64_t tasks = (uint64_t)nflag_max * d.M;
     const uint32_t grid = (uint32_t)(tasks < 148ull * 8 ? tasks : 148ull * 8);

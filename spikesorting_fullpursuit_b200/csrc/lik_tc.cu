@@ -962,7 +962,7 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
         FBP_CUDA(cudaMemsetAsync(P.wflag, 0, (size_t)d.nw * d.M, st));
     }
     FBP_CUDA(cudaMemsetAsync(&w.status()->n_fix, 0, 4, st));
-    FBP_CUDA(cudaFuncSetAttribute(lik_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    FBP_CUDA(allow_max_dyn_smem(lik_tc_kernel));
     const uint32_t grid = (uint32_t)((items + c.ntiles - 1) / c.ntiles);
     count_launch(2);
     {

@@ -881,7 +881,7 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     energy_table_kernel<<<(d.M * S2 + 255) / 256, 256, 0, st>>>(d, T, w.at<float2>(L.off_et));
     const size_t smem = (size_t)2 * d.C * d.W * 4 + 8 + (size_t)kLagChunk * (d.W + 1) * 8;
     if (smem > 200 * 1024) return fail(FBP_E_ARG, "template too large for the pair table kernel");
-    FBP_CUDA(cudaFuncSetAttribute(cross_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    FBP_CUDA(allow_max_dyn_smem(cross_table_kernel));
     cross_table_kernel<<<d.M * d.M, 256, smem, st>>>(d, T, w.at<float>(L.off_xt), w.at<float>(L.off_xtt),
                                                      w.at<float>(L.off_mx));
     energy_max_kernel<<<(d.M + 127) / 128, 128, 0, st>>>(d, w.at<float2>(L.off_et), w.at<float>(L.off_mx) + (size_t)d.M * d.M);
@@ -949,7 +949,7 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
     const bool bstaged = (uint64_t)d.M * S2 * 8 <= kBStage;
     const size_t smem_b = screen_smem_bytes(d.M, S2, bstaged);
     if (smem_b > 200 * 1024) return launch_overlap_plain(d, w, V, T, theta, nflag_max, st);
-    FBP_CUDA(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    FBP_CUDA(allow_max_dyn_smem(screen_kernel));
     const uint32_t groups = (d.M + Q - 1) / Q;
     float* G = w.at<float>(L.off_g);
     const float2* Et = w.at<float2>(L.off_et);
@@ -964,7 +964,7 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
         // persistent over the windows: as many CTAs as fit resident, split over the template groups
 #define FBP_PC(QQ)                                                                                            \
     case QQ: {                                                                                                \
-        FBP_CUDA(cudaFuncSetAttribute(partial_corr_kernel<QQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));                                                          \
+        FBP_CUDA(allow_max_dyn_smem(partial_corr_kernel<QQ>));                                                          \
         int per_sm = 1;                                                                                       \
         FBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, partial_corr_kernel<QQ>,              \
                                                                (int)pc_threads, smem_a));                 \
