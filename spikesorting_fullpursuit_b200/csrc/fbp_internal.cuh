@@ -145,6 +145,7 @@ struct Work {
 // a positive likelihood value recompute it exactly when its window row is flagged.
 struct LazyRef {
     const uint8_t* wflag;      // [nw][M] flags, or null: L is exact wherever read
+    const float* tnorm;        // [M][C] template channel norms (0: an all-zero channel, skipped)
     const float* V;
     const float* T;
     const float* bias;

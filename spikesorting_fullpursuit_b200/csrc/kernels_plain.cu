@@ -483,10 +483,11 @@ __global__ void __launch_bounds__(kOvThreads) overlap_plain_kernel(
 // Exact likelihood of (t, s) in the reference order (compute_maximum_likelihood,
 // binary_pursuit.cl:216-252) from the current voltage.
 __device__ float exact_lik(const Dims& d, const float* __restrict__ V, const float* __restrict__ T, float b,
-                           uint32_t t, uint32_t s)
+                           uint32_t t, uint32_t s, const float* __restrict__ tnorm)
 {
     float acc = b;
     for (uint32_t c = 0; c < d.C; ++c) {
+        if (tnorm[(uint64_t)t * d.C + c] == 0.f) continue;   // an all-zero template channel adds 0
         const float* tr = T + ((uint64_t)t * d.C + c) * d.W;
         const float* vr = V + (uint64_t)c * d.N + s;
         for (uint32_t j = 0; j < d.W; ++j) acc = fadd(acc, fmul(tr[j], vr[j]));
@@ -501,7 +502,7 @@ __device__ __forceinline__ float lik_value(const Dims& d, const float* __restric
                                            uint32_t s)
 {
     const float v = L[(uint64_t)t * d.N + s];
-    if (z.wflag != nullptr && v > 0.f && z.wflag[(uint64_t)(s / d.W) * d.M + t]) return exact_lik(d, z.V, z.T, z.bias[t], t, s);
+    if (z.wflag != nullptr && v > 0.f && z.wflag[(uint64_t)(s / d.W) * d.M + t]) return exact_lik(d, z.V, z.T, z.bias[t], t, s, z.tnorm);
     return v;
 }
 
@@ -961,9 +962,10 @@ int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint
 {
     if (nflag_max == 0) return FBP_OK;
     const uint32_t g = grid_for(nflag_max, 256);
-    LazyRef z{nullptr, V, T, bias};
+    LazyRef z{nullptr, nullptr, V, T, bias};
     if (lazy) {
         z.wflag = w.at<uint8_t>(w.lay->off_wflag);
+        z.tnorm = w.at<float>(w.lay->off_tnorm);
     }
     count_launch(5);
     parse_kernel<<<g, 256, 0, st>>>(d, w.L(), theta, w.flag(), w.status(), w.keys(), w.best_lik(),

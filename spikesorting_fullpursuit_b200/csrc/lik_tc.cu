@@ -182,11 +182,15 @@ __device__ __forceinline__ unsigned long long window_key(float v, uint32_t t, ui
     return ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - ((t << 10) | local_s));
 }
 
+// The reference's sum, skipping template channels that are entirely zero
+// (tnorm == 0): there it adds 0 * v terms, which leave a nonzero sum unchanged
+// (and a zero sum zero, up to the sign of zero, which no decision reads).
 __device__ float exact_likelihood(const Dims& d, const float* __restrict__ V, const float* __restrict__ T,
-                                  float b, uint32_t t, uint32_t s)
+                                  float b, uint32_t t, uint32_t s, const float* __restrict__ tnorm)
 {
     float acc = b;
     for (uint32_t c = 0; c < d.C; ++c) {
+        if (tnorm[(uint64_t)t * d.C + c] == 0.f) continue;
         const float* tr = T + ((uint64_t)t * d.C + c) * d.W;
         const float* vr = V + (uint64_t)c * d.N + s;
         for (uint32_t j = 0; j < d.W; ++j) acc = __fadd_rn(acc, __fmul_rn(tr[j], vr[j]));
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
                 const bool queued = local || (glob && g < P.fix_cap);
                 if (need && !queued) {
                     inline_done = true;
-                    return exact_likelihood(d, P.V, P.T, b, t, s);
+                    return exact_likelihood(d, P.V, P.T, b, t, s, P.tnorm);
                 }
                 return out;
             };
@@ -516,20 +520,28 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         const uint32_t k = lane & 3u;   // lanes 4..31 repeat lanes 0..3 and are discarded
         float acc = sbias[t];
         const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
+        // template channels that are entirely zero add 0 * v terms: skipped
+        const float* tnr = P.tnorm + (uint64_t)t * d.C;
+        auto next_active = [&](uint32_t c) {
+            while (c < d.C && tnr[c] == 0.f) ++c;
+            return c;
+        };
         float tv[4], tn[4];
+        uint32_t c = next_active(0);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const uint32_t x = lane + 32u * q;
-            tn[q] = x < W ? __ldg(tb + x) : 0.f;
+            tn[q] = (c < d.C && x < W) ? __ldg(tb + (uint64_t)c * Wp + x) : 0.f;
         }
-        for (uint32_t c = 0; c < d.C; ++c) {
+        while (c < d.C) {
+            const uint32_t cn = next_active(c + 1);
 #pragma unroll
             for (int q = 0; q < 4; ++q) tv[q] = tn[q];
-            if (c + 1 < d.C) {
+            if (cn < d.C) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const uint32_t x = lane + 32u * q;
-                    tn[q] = x < W ? __ldg(tb + (uint64_t)(c + 1) * Wp + x) : 0.f;
+                    tn[q] = x < W ? __ldg(tb + (uint64_t)cn * Wp + x) : 0.f;
                 }
             }
             const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0 + k;
@@ -544,6 +556,7 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
                     }
                 }
             }
+            c = cn;
         }
         if (lane < 4 && ((mask >> lane) & 1u)) {
             const uint32_t sk = t_s0[i] + r0 + lane;
@@ -602,7 +615,7 @@ __device__ __forceinline__ void note_window(const Dims& d, unsigned long long* w
 __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
                              const float* __restrict__ Tp, const float* __restrict__ bias,
                              const unsigned long long* __restrict__ fix, uint32_t cap, const DevStatus* status,
-                             float* L, unsigned long long* wkey, uint8_t* wpos)
+                             float* L, unsigned long long* wkey, uint8_t* wpos, const float* __restrict__ tnorm)
 {
     const uint32_t n = min(status->n_fix, cap);
     const uint32_t W = d.W, Wp = (W + 3) & ~3u, W4 = W & ~3u;
@@ -613,7 +626,7 @@ __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* _
         if ((uint64_t)s0 + W + 3 > d.N) {   // the run reaches the end of the chunk: one sample at a time
             for (uint32_t k = 0; k < 4; ++k)
                 if ((mask >> k) & 1u) {
-                    const float v = exact_likelihood(d, V, T, b, t, s0 + k);
+                    const float v = exact_likelihood(d, V, T, b, t, s0 + k, tnorm);
                     L[(uint64_t)t * d.N + s0 + k] = v;
                     note_window(d, wkey, wpos, v, t, s0 + k);
                 }
@@ -621,6 +634,7 @@ __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* _
         }
         float a0 = b, a1 = b, a2 = b, a3 = b;
         for (uint32_t c = 0; c < d.C; ++c) {
+            if (tnorm[(uint64_t)t * d.C + c] == 0.f) continue;   // an all-zero template channel adds 0
             const float* vr = V + (uint64_t)c * d.N + s0;
             const float* tr = Tp + ((uint64_t)t * d.C + c) * Wp;
             float w0 = __ldg(vr), w1 = __ldg(vr + 1), w2 = __ldg(vr + 2);   // V[s0 + j + 0..2]
@@ -706,7 +720,7 @@ __global__ void argmax_lazy_kernel(Dims d, const uint32_t* __restrict__ list, ui
 __global__ void lazy_fix_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
                                 const float* __restrict__ bias, const uint32_t* __restrict__ pidx,
                                 const DevStatus* status, const uint8_t* __restrict__ check, float* L,
-                                uint8_t* wflag)
+                                uint8_t* wflag, const float* __restrict__ tnorm)
 {
     const uint32_t n = status->n_spikes;
     for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
@@ -723,7 +737,7 @@ __global__ void lazy_fix_kernel(Dims d, const float* __restrict__ V, const float
                 const uint32_t q = (uint32_t)(a + e % (b - a));
                 if (!wflag[x * d.M + t]) continue;
                 float* lp = L + (uint64_t)t * d.N + q;
-                if (*lp > 0.f) *lp = exact_likelihood(d, V, T, bias[t], t, q);
+                if (*lp > 0.f) *lp = exact_likelihood(d, V, T, bias[t], t, q, tnorm);
             }
             __syncthreads();
             for (uint32_t t = threadIdx.x; t < d.M; t += blockDim.x) wflag[x * d.M + t] = 0;
@@ -876,7 +890,8 @@ int launch_lazy_fix(const Dims& d, const Work& w, const float* V, const float* T
     const Layout& L = *w.lay;
     count_launch();
     lazy_fix_kernel<<<std::min<uint32_t>(nmax, 148 * 16), 256, 0, st>>>(
-        d, V, T, bias, w.pidx(), w.status(), w.check(), w.L(), w.at<uint8_t>(L.off_wflag));
+        d, V, T, bias, w.pidx(), w.status(), w.check(), w.L(), w.at<uint8_t>(L.off_wflag),
+        w.at<float>(L.off_tnorm));
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }
@@ -970,7 +985,8 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
         lik_tc_kernel<<<grid, kThreads, c.smem, st>>>(P);
     }
     KScope ks(&fbp_chunk_stats::ms_fixup, st);
-    fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, P.Tp, bias, P.fix, P.fix_cap, w.status(), Lk, P.wkey, P.wpos);
+    fixup_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, P.Tp, bias, P.fix, P.fix_cap, w.status(), Lk, P.wkey, P.wpos,
+                                          P.tnorm);
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }

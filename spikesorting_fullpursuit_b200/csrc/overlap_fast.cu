@@ -324,13 +324,17 @@ __global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
 
 // Exact pair likelihood in the reference's float order (binary_pursuit.cl:578-632),
 // operands read from memory.
+// Channels on which both templates are entirely zero are skipped: there the
+// reference adds 0 * v and 0 * 0 terms, which leave its sums unchanged (acc
+// starts at +0, so no step of the reference makes it -0 either).
 __device__ float pair_exact_g(const Dims& d, const float* __restrict__ T, const float* __restrict__ V, uint32_t f,
-                              uint32_t t, uint32_t p, uint32_t a, uint32_t b)
+                              uint32_t t, uint32_t p, uint32_t a, uint32_t b, unsigned long long chans)
 {
     const int W = (int)d.W, fa = (int)d.S - (int)a, ta = (int)d.S - (int)b;
     const int jlo_f = max(0, -fa), jhi_f = min(W, W - fa), jlo_t = max(0, -ta), jhi_t = min(W, W - ta);
     float acc = 0.f;
     for (uint32_t c = 0; c < d.C; ++c) {
+        if (c < 64 && !((chans >> c) & 1ull)) continue;
         const float* fr = T + ((uint64_t)f * d.C + c) * d.W + fa;
         const float* tr = T + ((uint64_t)t * d.C + c) * d.W + ta;
         const float* vr = V + (uint64_t)c * d.N + p;
@@ -762,7 +766,7 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
                     const float ub = (R.uf + R.ua[x]) - xv;
                     if (!(ub >= thr)) continue;
                     const uint32_t a = R.fixed_a ? R.y : (uint32_t)x, b = R.fixed_a ? (uint32_t)x : R.y;
-                    const float v = pair_exact_g(d, T, V, f, R.t, p, a, b);
+                    const float v = pair_exact_g(d, T, V, f, R.t, p, a, b, mf | chmask[R.t]);
                     ++exact_n;
                     if (!(v > 0.f)) continue;
                     const uint64_t rr0 = (uint64_t)R.t + (uint64_t)M * a + (uint64_t)M * S2 * b;
@@ -826,7 +830,8 @@ __global__ void __launch_bounds__(256) score_kernel(Dims d, const float* __restr
                                                     const uint32_t* __restrict__ best_lab,
                                                     const uint32_t* __restrict__ best_idx,
                                                     const unsigned long long* __restrict__ gcand, uint32_t cap,
-                                                    DevStatus* status, unsigned long long* keys)
+                                                    DevStatus* status, unsigned long long* keys,
+                                                    const unsigned long long* __restrict__ chmask)
 {
     const uint32_t n = min(status->cand_count, cap);
     const uint32_t S2 = 2 * d.S + 1, M = d.M;
@@ -844,7 +849,7 @@ __global__ void __launch_bounds__(256) score_kernel(Dims d, const float* __restr
         if ((uint64_t)k0 + kk >= status->n_flag || t >= M || a >= S2 || b >= S2) continue;
         const uint32_t id = flag[k0 + kk];
         const uint32_t f = best_lab[id], p = best_idx[id];
-        const float acc = pair_exact_g(d, T, V, f, t, p, a, b);
+        const float acc = pair_exact_g(d, T, V, f, t, p, a, b, chmask[f] | chmask[t]);
         ++done;
         if (!(acc > 0.f)) continue;
         const uint64_t r = (uint64_t)t + (uint64_t)M * a + (uint64_t)M * S2 * b;
@@ -997,7 +1002,7 @@ int launch_overlap_fast(const Dims& d, const Work& w, const float* V, const floa
         }
         KScope ks(&fbp_chunk_stats::ms_score, st);
         score_kernel<<<148 * 8, 256, 0, st>>>(d, V, T, w.flag(), k0, w.best_lab(), w.best_idx(), gcand,
-                                              (uint32_t)L.cand_cap, w.status(), w.keys());
+                                              (uint32_t)L.cand_cap, w.status(), w.keys(), chm);
         FBP_CUDA(cudaGetLastError());
     }
     return FBP_OK;
