@@ -40,6 +40,7 @@ Differences, all documented:
 from __future__ import annotations
 
 import ctypes
+import os
 from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
@@ -126,8 +127,8 @@ class _Uploader:
     row-strided view: the float32 conversion happens in the slab copy."""
 
     SLAB_FLOATS = 4 << 20    # 16 MB per slab
-    N_SLABS = 8
-    N_THREADS = 4
+    N_SLABS = 16
+    N_THREADS = max(1, min(8, (os.cpu_count() or 2) // 2))
 
     def __init__(self, torch, dev):
         self.torch = torch

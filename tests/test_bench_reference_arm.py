@@ -14,7 +14,7 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
                     reason="reference kernels not built for the CPU")
 def test_reference_arm_line():
     out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "1", "--cpu-sample-s", "0.25"], capture_output=True, text=True,
+                          "--warmup", "1", "--cpu-sample-s", "0.25", "--duration", "2"], capture_output=True, text=True,
                          timeout=600, cwd=REPO)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
