@@ -802,12 +802,29 @@ __global__ void residual_parallel_kernel(Dims d, float* V, const float* __restri
     }
     __syncthreads();
     if (s_conf) return;
-    const uint32_t CW = d.C * d.W;
-    for (uint32_t e = threadIdx.x; e < CW; e += blockDim.x) {
-        const uint32_t c = e / d.W, j = e - c * d.W;
-        if (s + j >= d.N) continue;
-        float* vp = V + (uint64_t)c * d.N + s + j;
-        *vp = fsub(*vp, T[((uint64_t)l * d.C + c) * d.W + j]);
+    // one warp per channel row: the row's span [s, min(s+W, N)) is updated with
+    // 16-byte loads and stores over its 16-byte-aligned body, scalar at the ends
+    // (each element is still one float32 subtraction)
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const uint64_t end = s + d.W < d.N ? s + d.W : d.N;
+    for (uint32_t c = warp; c < d.C; c += nwarps) {
+        float* row = V + (uint64_t)c * d.N;
+        const float* tr = T + ((uint64_t)l * d.C + c) * d.W - s;   // tr[x] = T[l][c][x - s]
+        // first index at a 16-byte-aligned address (the row is float-aligned)
+        const uint64_t mis = (reinterpret_cast<uintptr_t>(row + s) >> 2) & 3u;
+        uint64_t a = s + ((4u - mis) & 3u);
+        a = a < end ? a : end;
+        const uint64_t b = a + ((end - a) & ~3ull);                    // end of the aligned body
+        for (uint64_t x = s + lane; x < a; x += 32) row[x] = fsub(row[x], tr[x]);
+        for (uint64_t x = a + 4ull * lane; x < b; x += 128) {
+            float4 v = *reinterpret_cast<float4*>(row + x);
+            v.x = fsub(v.x, tr[x]);
+            v.y = fsub(v.y, tr[x + 1]);
+            v.z = fsub(v.z, tr[x + 2]);
+            v.w = fsub(v.w, tr[x + 3]);
+            *reinterpret_cast<float4*>(row + x) = v;
+        }
+        for (uint64_t x = b + lane; x < end; x += 32) row[x] = fsub(row[x], tr[x]);
     }
 }
 
