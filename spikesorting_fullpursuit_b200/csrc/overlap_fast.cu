@@ -368,7 +368,6 @@ constexpr uint32_t kScreenGrid = 148 * 2;  // persistent CTAs (two per SM); also
 
 struct ScreenShared {
     float lb;
-    float nv;
     float maxau2;
     unsigned long long best;
     uint32_t nA;
@@ -381,7 +380,7 @@ struct ScreenShared {
 __host__ __device__ inline size_t screen_smem_bytes(uint32_t M, uint32_t S2, bool staged)
 {
     const size_t s2p = (S2 + 3) & ~3u, mp = (M + 3) & ~3u;
-    size_t b = 5 * s2p * 4 + 2 * mp * 4 + (size_t)kRowCap * 8 + (size_t)kCandCap * 12;
+    size_t b = 5 * s2p * 4 + 3 * mp * 4 + 256 * 4 + (size_t)kRowCap * 8 + (size_t)kCandCap * 12;
     b += (((size_t)S2 + 15) & ~(size_t)15) + (((size_t)M * S2 + 15) & ~(size_t)15);
     if (staged) b += (size_t)M * S2 * 8;
     return b + 64;
@@ -405,8 +404,9 @@ struct ScreenRow {
 //   rows, kind 2: (t, b) with L_t(b) > 0 -- b fixed, the lanes run over a not in A+
 //                 (transposed cross table XTT[f][t][b][:]).
 // Per window the CTA stages Bu/Bl[t][b] = G_t(b) +- beta_t(b) and Au/Al[a] =
-// G_f(a) +- alpha(a), with alpha + beta = K ((sqrt E_f(a) + sqrt E_t(b)) |v| +
+// G_f(a) +- alpha(a), with alpha + beta = K (sqrt E_f(a) |v|_f + sqrt E_t(b) |v|_t +
 // E_f(a) + E_t(b)) the rigorous bound of |estimate - reference float value|
+// (|v|_x: the window's norm over template x's non-zero channels)
 // (K carries slack for the few float operations of this regrouping).  Phase B
 // bounds every row from shared-memory maxima (each component at least the
 // item's, same monotone float order) and keeps the rows that can reach the
@@ -445,7 +445,9 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
     uint32_t* alist = reinterpret_cast<uint32_t*>(Al2 + s2p);   // [S2] A+ in ascending order
     float* gmaxu = reinterpret_cast<float*>(alist + s2p);       // [M] max_b Bu[t][b]
     float* nx = gmaxu + mp;                                     // [M] max -X_ft over items
-    float* rowmax = nx + mp;                                    // [kRowCap]
+    float* nvt = nx + mp;                                       // [M] window norm over template t's channels
+    float* vc2 = nvt + mp;                                      // [C <= 256] window energy per channel
+    float* rowmax = vc2 + 256;                                  // [kRowCap]
     uint32_t* rows = reinterpret_cast<uint32_t*>(rowmax + kRowCap);   // [kRowCap]
     uint32_t* cand = rows + kRowCap;                            // [kCandCap][3]
     uint8_t* fa = reinterpret_cast<uint8_t*>(cand + 3 * kCandCap);   // [S2] bit0 in bounds, bit1 L_f > 0
@@ -474,12 +476,19 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
         const float* Gk = G + (uint64_t)kk * M * S2;
         const unsigned long long mf = chmask[f];
         __syncthreads();
-        // ---- phase A: window quantities
-        float nv2 = 0.f;
-        for (uint32_t e = threadIdx.x; e < d.C * W; e += blockDim.x) {
-            const uint32_t c = e / W, j = e - c * W;
-            const float v = V[(uint64_t)c * d.N + p + j];
-            nv2 = fmaf(v, v, nv2);
+        // ---- phase A: window quantities.  The window's energy per channel gives,
+        // per template, the norm of the window over that template's channels: a
+        // template's products touch no other channel, so its part of the bound
+        // (Cauchy-Schwarz over its support) needs no more
+        for (uint32_t c = warp; c < d.C; c += nwarps) {
+            float e2 = 0.f;
+            for (uint32_t j = lane; j < W; j += 32) {
+                const float v = V[(uint64_t)c * d.N + p + j];
+                e2 = fmaf(v, v, e2);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, off);
+            if (lane == 0) vc2[c] = e2;
         }
         for (uint32_t x = threadIdx.x; x < S2; x += blockDim.x) {
             const uint64_t xp = (uint64_t)x + p;
@@ -487,20 +496,26 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
             fa[x] = inb ? ((L[(uint64_t)f * d.N + xp - S] > 0.f) ? 3 : 1) : 0;
         }
         for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) nx[t] = mx[(uint64_t)f * M + t];
-        const float nvs = RF(tmp.rf).Sum(nv2);
         if (threadIdx.x == 0) {
-            sh.nv = sqrtf(nvs) * 1.001f;
             sh.best = 0ull;
             sh.nrows = 0;
             sh.ncand = 0;
             sh.gfull = 0;
         }
         __syncthreads();
-        const float nv = sh.nv;
+        for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
+            const unsigned long long mt = chmask[t];   // all ones above 64 channels
+            float e2 = 0.f;
+            for (uint32_t c = 0; c < d.C; ++c)
+                if (c >= 64 || ((mt >> c) & 1ull)) e2 += vc2[c];
+            nvt[t] = sqrtf(e2) * 1.001f;
+        }
+        __syncthreads();
+        const float nvf = nvt[f];
         float ma2 = -INFINITY;
         for (uint32_t x = threadIdx.x; x < S2; x += blockDim.x) {
             const float2 ea = Etab[(uint64_t)f * S2 + x];
-            const float al = K * fmaf(nv, ea.y, ea.x);
+            const float al = K * fmaf(nvf, ea.y, ea.x);
             const float g = Gk[(uint64_t)f * S2 + x];
             const uint8_t fl = fa[x];
             const float au = (fl & 1) ? g + al : -INFINITY, alo = (fl & 1) ? g - al : -INFINITY;
@@ -516,7 +531,7 @@ __global__ void __launch_bounds__(kScrThreads, 2) screen_kernel(
             const uint64_t xp = (uint64_t)x + p;
             const bool inb = xp >= S && xp < (uint64_t)d.N - W + S;
             const float2 eb = Etab[e];
-            const float be = K * fmaf(nv, eb.y, eb.x);
+            const float be = K * fmaf(nvt[t], eb.y, eb.x);
             const float g = Gk[e];
             Bu[e] = inb ? g + be : -INFINITY;
             Bl[e] = inb ? g - be : -INFINITY;

@@ -5,7 +5,8 @@ For items (a, t, b) of flagged-style windows, the reference's own float32 pair v
 interval the screen computes from its estimate:
     LB = (Al[a] + Bl[t][b]) - X,   UB = (Au[a] + Bu[t][b]) - X
     Au/Al = G_f(a) +- alpha(a),  Bu/Bl = G_t(b) +- beta_t(b),
-    alpha + beta = K ((sqrt E_f + sqrt E_t) |v| + E_f + E_t),
+    alpha + beta = K (sqrt E_f |v|_f + sqrt E_t |v|_t + E_f + E_t),
+    |v|_x = the window's norm over template x's non-zero channels,
     K = 1.01 * 1.05 * 2 (C W + C + W + 24) 2^-24
 with the partial correlations G summed in float32 in an order unlike the reference's
 (numpy's pairwise reduction), the truncated energies rounded up and the cross terms X
@@ -50,9 +51,14 @@ def test_reference_pair_values_lie_inside_the_screen_interval():
     keep = (onsets >= S) & (onsets + S + W < N)
     onsets, labels = onsets[keep], truth["labels"][keep]
     checked = 0
+    chans = [np.flatnonzero(np.any(T[t] != 0, axis=1)) for t in range(M)]
+    tighter = []
     for p, f in zip(onsets[:4], labels[:4]):
         v = V[:, p:p + W]
-        nv = f32(np.sqrt((v.astype(np.float64) ** 2).sum()) * 1.001)
+        vc2 = (v.astype(np.float64) ** 2).sum(axis=1)
+        nv_all = f32(np.sqrt(vc2.sum()) * 1.001)
+        nv = [f32(np.sqrt(vc2[chans[t]].sum()) * 1.001) for t in range(M)]
+        tighter += [float(nv[t] / nv_all) for t in range(M)]
         shifts = np.unique(np.concatenate([np.arange(S - 3, S + 4), rng.integers(0, S2, 20)]))
         G, Es = {}, {}
         for t in range(M):
@@ -70,7 +76,7 @@ def test_reference_pair_values_lie_inside_the_screen_interval():
             Fa, Tb = _trunc(T, C, W, S, int(f), a), _trunc(T, C, W, S, t, b)
             X = f32((Fa.astype(np.float64) * Tb.astype(np.float64)).sum())
             (Ef, sEf), (Et, sEt) = Es[(int(f), a)], Es[(t, b)]
-            al, be = K * (nv * sEf + Ef), K * (nv * sEt + Et)
+            al, be = K * (nv[int(f)] * sEf + Ef), K * (nv[t] * sEt + Et)
             Au, Al = G[(int(f), a)] + al, G[(int(f), a)] - al
             Bu, Bl = G[(t, b)] + be, G[(t, b)] - be
             ub, lb = f32(f32(Au + Bu) - X), f32(f32(Al + Bl) - X)
@@ -78,3 +84,5 @@ def test_reference_pair_values_lie_inside_the_screen_interval():
             assert lb <= ref <= ub, (int(p), int(f), t, a, b, float(lb), ref, float(ub))
             checked += 1
     assert checked > 1000
+    # templates on 4-6 of 16 channels: the per-template norms are well below the window's
+    assert np.mean(tighter) < 0.8
