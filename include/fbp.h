@@ -93,7 +93,7 @@ typedef struct fbp_chunk_stats {
  * partial correlations; 0 leaves a choice to the library.  Values the sizes do
  * not allow (shared memory, TMEM) fall back to the library's choice. */
 typedef struct fbp_tuning {
-    uint32_t lik_tiles;    /* 128-sample tiles per likelihood CTA: 1 or 2 */
+    uint32_t lik_tiles;    /* 128-sample tiles per likelihood CTA: 1 to 4 */
     uint32_t lik_group;    /* (tap, channel pair) steps of templates per staged copy */
     uint32_t lik_stages;   /* staged template copies in flight: 2 to 8 */
     uint32_t pc_group;     /* templates per partial-correlation CTA: 1, 2, 4 or 8 */

@@ -87,7 +87,7 @@ def _time(torch, fn, reps=3):
 
 def lik_candidates(M):
     Np = (M + 15) // 16 * 16
-    tiles = (2, 1) if Np <= 128 else (1,)
+    tiles = tuple(k for k in (2, 4, 1) if k * Np <= 512)
     out = []
     for lt in tiles:
         for st in (0, 4, 6):

@@ -199,7 +199,7 @@ extern "C" int fbp_set_tuning(const fbp_tuning* t)
         tuning() = fbp_tuning{};
         return FBP_OK;
     }
-    if (t->lik_tiles > 2 || (t->lik_stages != 0 && (t->lik_stages < 2 || t->lik_stages > 8)) ||
+    if (t->lik_tiles > 4 || (t->lik_stages != 0 && (t->lik_stages < 2 || t->lik_stages > 8)) ||
         (t->pc_group != 0 && t->pc_group != 1 && t->pc_group != 2 && t->pc_group != 4 && t->pc_group != 8) ||
         t->lik_group > 64)
         return fail(FBP_E_ARG, "tuning value out of range");

@@ -830,7 +830,7 @@ bool tc_config(const Dims& d, TcConfig* c)
     // or one tile); above 128 columns one tile per CTA and two CTAs per SM
     c->ntiles = c->Np <= 128 ? 2 : 1;
     const fbp_tuning& tu = tuning();
-    if (tu.lik_tiles == 1) c->ntiles = 1;
+    if (tu.lik_tiles >= 1 && tu.lik_tiles <= 4 && tu.lik_tiles * c->Np <= 512) c->ntiles = tu.lik_tiles;
     for (;;) {
         const uint32_t cols = c->ntiles * c->Np;
         c->ncols = 32;

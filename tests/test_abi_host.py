@@ -127,7 +127,7 @@ def test_adjoint_arguments_fail_before_any_device_call(lib):
 
 
 def test_tuning_validation(lib):
-    t = _native.FbpTuning(3, 0, 0, 0)   # more than two tiles per CTA
+    t = _native.FbpTuning(5, 0, 0, 0)   # more than four tiles per CTA
     assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
     t = _native.FbpTuning(0, 0, 9, 0)   # ring deeper than 8
     assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
