@@ -5,9 +5,9 @@ fbp_tuning): 128-sample tiles per tensor-core likelihood CTA, template steps
 per staged copy, staged copies in flight, and templates per
 partial-correlation CTA.  ``tune`` measures candidates on the caller's own
 data -- a leading slice of the voltage with the real templates -- and keeps
-the fastest: first the likelihood shapes, timing the likelihood of every
-window of the slice (fbp_likelihood), then the partial-correlation group,
-timing whole pursuits of the slice.  Results are cached in a JSON file
+the fastest: first the likelihood shapes, by the likelihood kernel's device
+time within whole pursuits of the slice (the pass-by-pass window lists of a
+real pursuit), then the partial-correlation group, by whole pursuits.  Results are cached in a JSON file
 (``FBP_TUNE_CACHE``, else ~/.cache/spikesorting_fullpursuit_b200/tuning.json)
 keyed by (channels, templates, window, shift, device name), so each shape is
 measured once.  Launch shapes change speed only: every candidate gives the
@@ -128,40 +128,35 @@ def tune(voltage, templates, bias, theta, W, S, overlap=True, sample_s=None, sam
     d = _native.dims(C, n, M, W, S)
     flags = _native.FBP_OVERLAP_RECHECK if overlap else 0
     ws = torch.empty(_native.workspace_bytes(d, flags), dtype=torch.uint8, device=dev)
-    lik = torch.empty((M, n), dtype=torch.float32, device=dev)
     stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    Vw = torch.empty_like(V0)
+    cap = 8 * (n // W + 1) + 1024
+    idx = torch.empty(cap, dtype=torch.int32, device=dev)
+    lab = torch.empty(cap, dtype=torch.int32, device=dev)
 
-    def run_lik():
-        _native.check(L.fbp_likelihood(ctypes.byref(d), 1, _ptr(V0), _ptr(T), _ptr(b), None, 0, _ptr(lik), _ptr(ws),
-                                       ws.numel(), stream))
+    def run_pursuit(timing):
+        Vw.copy_(V0)
+        k = ctypes.c_uint32(0)
+        st = _native.FbpChunkStats()
+        _native.check(L.fbp_pursue_chunk(ctypes.byref(d), flags | (_native.FBP_TIMING if timing else 0), _ptr(Vw),
+                                         _ptr(T), _ptr(b), _ptr(th), _ptr(ws), ws.numel(), _ptr(idx), _ptr(lab), cap,
+                                         ctypes.byref(k), ctypes.byref(st), 0, stream))
+        return st
 
     best, best_ms = None, None
     try:
         for cand in lik_candidates(M):
             apply(cand)
-            run_lik()   # warm
-            ms = _time(torch, run_lik)
+            ms = min(run_pursuit(True).ms_lik_tc for _ in range(2))
             if best_ms is None or ms < best_ms:
                 best, best_ms = dict(cand), ms
         if overlap:
-            Vw = torch.empty_like(V0)
-            cap = 8 * (n // W + 1) + 1024
-            idx = torch.empty(cap, dtype=torch.int32, device=dev)
-            lab = torch.empty(cap, dtype=torch.int32, device=dev)
-
-            def run_pursuit():
-                Vw.copy_(V0)
-                k = ctypes.c_uint32(0)
-                _native.check(L.fbp_pursue_chunk(ctypes.byref(d), flags, _ptr(Vw), _ptr(T), _ptr(b), _ptr(th),
-                                                 _ptr(ws), ws.numel(), _ptr(idx), _ptr(lab), cap, ctypes.byref(k),
-                                                 None, 0, stream))
-
             pbest, pbest_ms = None, None
             for q in (0, 8, 4, 2):
                 cand = dict(best, pc_group=q)
                 apply(cand)
-                run_pursuit()
-                ms = _time(torch, run_pursuit, reps=2)
+                run_pursuit(False)
+                ms = _time(torch, lambda: run_pursuit(False), reps=2)
                 if pbest_ms is None or ms < pbest_ms:
                     pbest, pbest_ms = cand, ms
             best = pbest
