@@ -601,6 +601,447 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
 // set.  A thread carries the four samples' sequential sums side by side: per 4
 // taps one 16-byte template load and 4 voltage loads feed 16 multiply-adds
 // (each sum still adds its products one at a time, in the reference's order).
+// ---------------------------------------------------------------------------
+// Persistent tensor-core likelihood (the pursuit's passes, lazy exactness).
+//
+// One CTA per SM walks batches of B tiles.  The voltage strips and the TMEM
+// accumulators are double-buffered, so while the 4 epilogue warps finish batch
+// k (estimates, bounds, window maxima, exact recomputation of the queued runs
+// from the strips, window keys), the bulk-copy warp and the MMA warp already run
+// batch k+1; and each pass of the template ring feeds B tiles (as many as one
+// TMEM buffer of 256 columns holds) instead of one CTA's two.
+//   barriers: a_full[s]   strips (and the batch's tile list) of buffer s loaded
+//             a_empty[s]  the epilogue is done with buffer s's strips
+//             acc_full[s] the MMAs of buffer s's batch completed (tcgen05.commit)
+//             acc_empty[s] the epilogue has read TMEM buffer s
+//             b_full/b_empty  the template ring, stage counter running across batches
+// The results are those of lik_tc_kernel in lazy mode.
+// ---------------------------------------------------------------------------
+// True on every epilogue thread (named barrier 1, 128 threads) iff p holds on
+// all of them: the epilogue's loop decisions stay uniform, so no thread leaves a
+// loop whose named barriers the others still wait at.
+__device__ __forceinline__ bool epi_all(bool p)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, 1, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)p)
+        : "memory");
+    return r != 0;
+}
+
+struct PersistParams {
+    TcParams P;          // sizes, tensors, bounds, outputs (P.ntiles = tiles per batch)
+    uint32_t nbatches;
+};
+
+__global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistParams Q)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const TcParams& P = Q.P;
+    const Dims& d = P.d;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t B = P.ntiles;
+    const uint32_t strip_bytes = P.R8 * 16;
+    const uint32_t tile_bytes = P.Cq * strip_bytes;
+    const uint32_t kstep_bytes = P.Np * 32;
+    const uint32_t stage_bytes = P.group * kstep_bytes;
+    unsigned char* A = smem;                                       // [2][B][tile]
+    unsigned char* R = A + 2 * B * tile_bytes;                     // template ring
+    uint64_t* bars = reinterpret_cast<uint64_t*>(R + P.stages * stage_bytes);
+    uint64_t* a_full = bars;          // [2]
+    uint64_t* a_empty = bars + 2;     // [2]
+    uint64_t* acc_full = bars + 4;    // [2]
+    uint64_t* acc_empty = bars + 6;   // [2]
+    uint64_t* drain = bars + 8;       // the MMA warp's last commit, on an error
+    uint64_t* b_full = bars + 9;
+    uint64_t* b_empty = b_full + P.stages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(b_empty + P.stages);
+    uint32_t* err = tmem_slot + 1;
+    uint32_t* meta = err + 1;                                      // [2][3][B]: s0, rows, first window
+    float* snorm = reinterpret_cast<float*>(meta + 6 * B);         // [B][C]
+    float* bnd = snorm + B * d.C;                                  // [B][M]
+    float* sbias = bnd + B * d.M;                                  // [M]
+    uint32_t* fq = reinterpret_cast<uint32_t*>(sbias + d.M);       // [kFixCap]: t << 14 | tile << 11 | row << 4 | mask
+    uint32_t* nfq = fq + kFixCap;
+    int* s_mlb = reinterpret_cast<int*>(nfq + 1);                  // [B][wslots]
+    uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_mlb + B * P.wslots);
+    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(
+        (reinterpret_cast<uintptr_t>(s_pos + B * P.wslots) + 7) & ~(uintptr_t)7);
+    uint8_t* s_inex = reinterpret_cast<uint8_t*>(s_key + B * P.wslots);   // [B][wslots][M]
+
+    const uint32_t ksteps = d.W * (P.Cq / 2);
+    const uint32_t ngroups = (ksteps + P.group - 1) / P.group;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&a_full[s], 1);
+            mbar_init(&a_empty[s], 1);
+            mbar_init(&acc_full[s], 1);
+            mbar_init(&acc_empty[s], 1);
+        }
+        for (uint32_t s = 0; s < P.stages; ++s) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1);
+        }
+        mbar_init(drain, 1);
+        *err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (uint32_t t = threadIdx.x; t < d.M; t += blockDim.x) sbias[t] = P.bias[t];
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(512u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t gtot = 0;
+            for (uint32_t batch = blockIdx.x, it = 0; batch < Q.nbatches; batch += gridDim.x, ++it) {
+                const uint32_t s = it & 1, use = it >> 1;
+                if (*(volatile uint32_t*)err) break;
+                if (use > 0 && !mbar_wait(&a_empty[s], (use - 1) & 1)) { atomicOr(err, 1u); break; }
+                uint32_t* ms0 = meta + s * 3 * B;
+                uint32_t* mrows = ms0 + B;
+                uint32_t* mw0 = mrows + B;
+                for (uint32_t i = 0; i < B; ++i) {
+                    const uint64_t item = (uint64_t)batch * B + i;
+                    uint32_t s0 = 0, rows = 0;
+                    if (P.list == nullptr) {
+                        const uint64_t st = item * kTile;
+                        if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)kTile ? d.N - st : (uint64_t)kTile); }
+                    } else if (item < P.nitems) {
+                        const uint64_t st = (uint64_t)P.list[item] * d.W;
+                        if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)d.W ? d.N - st : (uint64_t)d.W); }
+                    }
+                    ms0[i] = s0;
+                    mrows[i] = rows;
+                    mw0[i] = s0 / d.W;
+                }
+                unsigned char* Ab = A + s * B * tile_bytes;
+                mbar_expect_tx(&a_full[s], B * tile_bytes);
+                for (uint32_t i = 0; i < B; ++i)
+                    for (uint32_t q = 0; q < P.Cq; ++q)
+                        bulk_g2s(Ab + i * tile_bytes + q * strip_bytes, P.Vq + ((uint64_t)q * P.rows + ms0[i]) * 4,
+                                 strip_bytes, &a_full[s]);
+                bool ok = true;
+                for (uint32_t g = 0; g < ngroups; ++g, ++gtot) {
+                    const uint32_t st = gtot % P.stages, round = gtot / P.stages;
+                    if (round > 0 && !mbar_wait(&b_empty[st], (round - 1) & 1)) { ok = false; break; }
+                    const uint32_t k0 = g * P.group, nk = min(P.group, ksteps - k0);
+                    mbar_expect_tx(&b_full[st], nk * kstep_bytes);
+                    bulk_g2s(R + st * stage_bytes, P.Tq + (uint64_t)k0 * P.Np * 8, nk * kstep_bytes, &b_full[st]);
+                }
+                if (!ok) { atomicOr(err, 1u); break; }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((P.Np >> 3) << 17) | ((kTile >> 4) << 24);
+            const uint32_t r_base = smem_u32(R);
+            uint32_t gtot = 0;
+            for (uint32_t batch = blockIdx.x, it = 0; batch < Q.nbatches; batch += gridDim.x, ++it) {
+                const uint32_t s = it & 1, use = it >> 1;
+                if (*(volatile uint32_t*)err) break;
+                if (!mbar_wait(&a_full[s], use & 1)) { atomicOr(err, 2u); break; }
+                if (use > 0 && !mbar_wait(&acc_empty[s], (use - 1) & 1)) { atomicOr(err, 2u); break; }
+                tc_fence_after();
+                const uint32_t a_base = smem_u32(A + s * B * tile_bytes);
+                const uint32_t dcol = tmem + s * 256u;
+                bool ok = true;
+                for (uint32_t g = 0; g < ngroups; ++g, ++gtot) {
+                    const uint32_t st = gtot % P.stages, round = gtot / P.stages;
+                    if (!mbar_wait(&b_full[st], round & 1)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t k0 = g * P.group, nk = min(P.group, ksteps - k0);
+                    for (uint32_t kq = 0; kq < nk; ++kq) {
+                        const uint32_t k = k0 + kq;
+                        const uint32_t j = k / (P.Cq / 2), qp = k % (P.Cq / 2);
+                        const uint64_t bdesc = umma_desc(r_base + st * stage_bytes + kq * kstep_bytes, P.Np * 16, 128);
+                        for (uint32_t i = 0; i < B; ++i) {
+                            const uint32_t a_addr = a_base + i * tile_bytes + (2 * qp) * strip_bytes + j * 16;
+                            umma_tf32(dcol + i * P.Np, umma_desc(a_addr, strip_bytes, 128), bdesc, idesc, k > 0 ? 1u : 0u);
+                        }
+                    }
+                    umma_commit(&b_empty[st]);
+                }
+                umma_commit(&acc_full[s]);   // completes once every MMA issued so far has
+                if (!ok) { atomicOr(err, 2u); break; }
+            }
+        }
+    } else {
+        const uint32_t et = threadIdx.x - 64, ew = warp - 2;   // 128 epilogue threads, warps 0..3
+        const uint32_t qd = warp & 3, row = qd * 32 + lane;
+        for (uint32_t batch = blockIdx.x, it = 0; batch < Q.nbatches; batch += gridDim.x, ++it) {
+            const uint32_t s = it & 1, use = it >> 1;
+            if (!epi_all(*(volatile uint32_t*)err == 0)) break;
+            if (!epi_all(mbar_wait(&a_full[s], use & 1))) { if (et == 0) atomicOr(err, 4u); break; }
+            const uint32_t* t_s0 = meta + s * 3 * B;
+            const uint32_t* t_rows = t_s0 + B;
+            const uint32_t* t_w0 = t_rows + B;
+            unsigned char* Ab = A + s * B * tile_bytes;
+            // per-batch scratch, norms of the strips and the bounds
+            if (et == 0) *nfq = 0;
+            for (uint32_t e = et; e < B * P.wslots; e += 128) {
+                s_mlb[e] = 0;
+                s_pos[e] = 0;
+                s_key[e] = 0ull;
+            }
+            for (uint32_t e = et; e < B * P.wslots * d.M; e += 128) s_inex[e] = 0;
+            for (uint32_t e = et; e < B * d.C; e += 128) {
+                const uint32_t i = e / d.C, c = e % d.C;
+                const float* col = reinterpret_cast<const float*>(Ab + i * tile_bytes + (c / 4) * strip_bytes) + (c % 4);
+                const uint32_t nr = t_rows[i] ? t_rows[i] + d.W - 1 : 0;
+                float acc = 0.f;
+                for (uint32_t r = 0; r < nr; ++r) acc = fmaf(col[r * 4], col[r * 4], acc);
+                snorm[e] = sqrtf(acc) * 1.0001f;
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            for (uint32_t e = et; e < B * d.M; e += 128) {
+                const uint32_t i = e / d.M, t = e % d.M;
+                float a = 0.f;
+                for (uint32_t c = 0; c < d.C; ++c) a = fmaf(P.tnorm[t * d.C + c], snorm[i * d.C + c], a);
+                bnd[e] = P.k_a * a * 1.0001f + P.k_b * fabsf(sbias[t]);
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (!epi_all(mbar_wait(&acc_full[s], use & 1))) { if (et == 0) atomicOr(err, 8u); break; }
+            tc_fence_after();
+            const uint32_t tbase = tmem + ((qd * 32) << 16) + s * 256u;
+            auto enqueue = [&](bool need, uint32_t t, uint32_t i, uint32_t sm_, float b, float out, bool& here) {
+                here = false;
+                const uint32_t m = __ballot_sync(0xffffffffu, need);
+                if (m == 0u) return out;
+                uint32_t nz = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                const uint32_t k = lane >> 2;
+                const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
+                const uint32_t nib = (m >> (4 * k)) & 0xFu;
+                const bool local = nib && slot < kFixCap;
+                if ((lane & 3u) == 0 && local) fq[slot] = (t << 14) | (i << 11) | (row << 4) | nib;
+                const bool glob = nib && !local;
+                uint32_t g = 0;
+                if (glob && (lane & 3u) == 0) {
+                    g = atomicAdd(&P.status->n_fix, 1u);
+                    if (g < P.fix_cap)
+                        P.fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | sm_;
+                }
+                g = __shfl_sync(0xffffffffu, g, lane & ~3u);
+                const bool queued = local || (glob && g < P.fix_cap);
+                if (need && !queued) {
+                    here = true;
+                    return exact_likelihood(d, P.V, P.T, b, t, sm_, P.tnorm);
+                }
+                return out;
+            };
+            auto note_exact = [&](float v, uint32_t t, uint32_t i, uint32_t sm_, const uint32_t* w0) {
+                if (!(v > 0.f)) return;
+                const uint32_t w = sm_ / d.W, slot = i * P.wslots + (w - w0[i]);
+                atomicMax(&s_key[slot], window_key(v, t, sm_ - w * d.W));
+                s_pos[slot] = 1u;
+            };
+            // pass 1: estimates, samples of uncertain sign, the window's largest lower bound
+            for (uint32_t i = 0; i < B; ++i) {
+                const uint32_t sm_ = t_s0[i] + row;
+                const bool valid = row < t_rows[i];
+                const bool live = valid && (uint64_t)sm_ + d.W < d.N;
+                const uint32_t wslot = valid ? i * P.wslots + (sm_ / d.W - t_w0[i]) : 0u;
+                for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
+                    float v[16];
+                    tmem_ld16(tbase + i * P.Np + cg * 16, v);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const uint32_t t = cg * 16 + e;
+                        if (t >= d.M) continue;
+                        const float b = sbias[t];
+                        const float est = v[e] + b;
+                        const float bd = bnd[i * d.M + t];
+                        const bool certain = live && est - bd > 0.f;
+                        const bool need = live && !(est + bd <= 0.f) && !certain;
+                        if (certain) {
+                            atomicMax(&s_mlb[wslot], __float_as_int(est - bd));
+                            s_pos[wslot] = 1u;
+                        }
+                        bool here = false;
+                        const float out = enqueue(need, t, i, sm_, b, live ? est : 0.f, here);
+                        if (here) note_exact(out, t, i, sm_, t_w0);
+                        if (valid) P.L[(uint64_t)t * d.N + sm_] = out;
+                    }
+                }
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            // pass 2: contenders for each window's maximum are recomputed; the other
+            // certainly positive samples keep their estimate, their window row flagged
+            for (uint32_t i = 0; i < B; ++i) {
+                const uint32_t sm_ = t_s0[i] + row;
+                const bool valid = row < t_rows[i];
+                const bool live = valid && (uint64_t)sm_ + d.W < d.N;
+                const uint32_t wslot = valid ? i * P.wslots + (sm_ / d.W - t_w0[i]) : 0u;
+                const float mlb = __int_as_float(s_mlb[wslot]);
+                for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
+                    float v[16];
+                    tmem_ld16(tbase + i * P.Np + cg * 16, v);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const uint32_t t = cg * 16 + e;
+                        if (t >= d.M) continue;
+                        const float b = sbias[t];
+                        const float est = v[e] + b;
+                        const float bd = bnd[i * d.M + t];
+                        const bool certain = live && est - bd > 0.f;
+                        const bool contender = certain && est + bd >= mlb;
+                        bool here = false;
+                        const float out = enqueue(contender, t, i, sm_, b, est, here);
+                        if (here) {
+                            note_exact(out, t, i, sm_, t_w0);
+                            P.L[(uint64_t)t * d.N + sm_] = out;
+                        }
+                        if (certain && !contender) s_inex[wslot * d.M + t] = 1;
+                    }
+                }
+            }
+            // TMEM buffer s read: the MMAs of batch it+2 may use it
+            tc_fence_before();
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (et == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[s])) : "memory");
+            // exact recomputation of the queued runs from buffer s's strips, transposed in
+            // place to channel-major rows (the MMAs of this batch are complete)
+            const uint32_t nq = min(*nfq, kFixCap);
+            if (et == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
+            const uint32_t Cp = P.Cq * 4;
+            if (nq > 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                constexpr uint32_t kPer = 2;   // R8 <= 256 rows <= kPer * 128
+                const float4* src = reinterpret_cast<const float4*>(Ab);
+                float* dst = reinterpret_cast<float*>(Ab);
+                for (uint32_t tq = 0; tq < B * P.Cq; ++tq) {
+                    float4 vv[kPer];
+#pragma unroll
+                    for (uint32_t k = 0; k < kPer; ++k) {
+                        const uint32_t r = k * 128 + et;
+                        vv[k] = r < P.R8 ? src[(size_t)tq * P.R8 + r] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                    asm volatile("bar.sync 1, 128;" ::: "memory");
+#pragma unroll
+                    for (uint32_t k = 0; k < kPer; ++k) {
+                        const uint32_t r = k * 128 + et;
+                        if (r >= P.R8) continue;
+                        float* o = dst + (size_t)4 * tq * P.R8 + r;
+                        o[0] = vv[k].x;
+                        o[P.R8] = vv[k].y;
+                        o[2 * P.R8] = vv[k].z;
+                        o[3 * P.R8] = vv[k].w;
+                    }
+                    asm volatile("bar.sync 1, 128;" ::: "memory");
+                }
+            }
+            const uint32_t W = d.W, Wp = (W + 3) & ~3u;
+            const float* Vt = reinterpret_cast<const float*>(Ab);
+            for (uint32_t qi = ew; qi < nq; qi += 4) {
+                const uint32_t e = fq[qi];
+                const uint32_t t = e >> 14, i = (e >> 11) & 7u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
+                const uint32_t k = lane & 3u;
+                float acc = sbias[t];
+                const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
+                const float* tnr = P.tnorm + (uint64_t)t * d.C;
+                auto next_active = [&](uint32_t c) {
+                    while (c < d.C && tnr[c] == 0.f) ++c;
+                    return c;
+                };
+                float tv[4], tn[4];
+                uint32_t c = next_active(0);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t x = lane + 32u * q;
+                    tn[q] = (c < d.C && x < W) ? __ldg(tb + (uint64_t)c * Wp + x) : 0.f;
+                }
+                while (c < d.C) {
+                    const uint32_t cn = next_active(c + 1);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) tv[q] = tn[q];
+                    if (cn < d.C) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const uint32_t x = lane + 32u * q;
+                            tn[q] = x < W ? __ldg(tb + (uint64_t)cn * Wp + x) : 0.f;
+                        }
+                    }
+                    const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0 + k;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+                        for (int jj = 0; jj < 32; ++jj) {
+                            const uint32_t j = 32u * q + jj;
+                            if (j < W) {
+                                const float tj = __shfl_sync(0xffffffffu, tv[q], jj);
+                                acc = __fadd_rn(acc, __fmul_rn(tj, vr[j]));
+                            }
+                        }
+                    }
+                    c = cn;
+                }
+                if (lane < 4 && ((mask >> lane) & 1u)) {
+                    const uint32_t sk = t_s0[i] + r0 + lane;
+                    P.L[(uint64_t)t * d.N + sk] = acc;
+                    if (acc > 0.f) {
+                        const uint32_t w = sk / W, slot = i * P.wslots + (w - t_w0[i]);
+                        atomicMax(&s_key[slot], window_key(acc, t, sk - w * W));
+                        s_pos[slot] = 1u;
+                    }
+                }
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            // publish the batch's window maxima, positive flags and estimate flags
+            for (uint32_t e = et; e < B * P.wslots; e += 128) {
+                const uint32_t i = e / P.wslots, j = e - i * P.wslots;
+                if (t_rows[i] == 0 || j > (t_s0[i] + t_rows[i] - 1) / W - t_w0[i]) continue;
+                const uint32_t w = t_w0[i] + j;
+                if (P.list != nullptr) {
+                    P.wkey[w] = s_key[e];
+                    P.wpos[w] = (uint8_t)(s_pos[e] ? 1 : 0);
+                } else {
+                    if (s_key[e]) atomicMax(&P.wkey[w], s_key[e]);
+                    if (s_pos[e]) P.wpos[w] = 1;
+                }
+            }
+            for (uint32_t e = et; e < B * P.wslots * d.M; e += 128) {
+                const uint32_t slot = e / d.M, t = e - slot * d.M;
+                const uint32_t i = slot / P.wslots, j = slot - i * P.wslots;
+                if (t_rows[i] == 0 || j > (t_s0[i] + t_rows[i] - 1) / W - t_w0[i]) continue;
+                const uint8_t f = s_inex[e];
+                if (P.list != nullptr || f) P.wflag[(uint64_t)(t_w0[i] + j) * d.M + t] = f;
+            }
+            // strips of buffer s (written through the generic proxy by the transposition)
+            // go back to the bulk copies
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (et == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&a_empty[s])) : "memory");
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *err) atomicOr(&P.status->error, 0x200u | *err);
+    if (warp == 1) {
+        if (lane == 0 && *err) {
+            // MMAs may still be in flight: a last commit arrives once all are done
+            umma_commit(drain);
+            mbar_wait(drain, 0);
+        }
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
+    }
+}
+
 // With lazy exactness, each positive exact value also enters its window's key
 // and positive flag (after the likelihood kernel has published the CTA's own).
 __device__ __forceinline__ void note_window(const Dims& d, unsigned long long* wkey, uint8_t* wpos, float v,
@@ -926,6 +1367,39 @@ int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const
     return FBP_OK;
 }
 
+// Persistent launch shape: tiles per batch (one TMEM buffer of 256 columns) and
+// the deepest template ring that fits the shared memory.  False when one buffer
+// holds fewer than two tiles or the caller asked for a tile count.
+struct PersistConfig {
+    uint32_t B, stages, group;
+    size_t smem;
+};
+
+bool persist_config(const Dims& d, const TcConfig& c, PersistConfig* p)
+{
+    if (tuning().lik_tiles != 0) return false;
+    uint32_t B = std::min<uint32_t>(8, 256 / c.Np);
+    if (B < 2) return false;
+    const size_t tile = (size_t)c.Cq * c.R8 * 16, kstep = (size_t)c.Np * 32;
+    const uint32_t ws = win_slots(d.W);
+    for (; B >= 2; --B) {
+        const size_t misc = (9 + 0) * 8 + 8 + 6 * B * 4 + (size_t)B * (d.C + d.M) * 4 + (size_t)d.M * 4 +
+                            (size_t)kFixCap * 4 + 4 + (size_t)B * ws * 8 + 8 + (size_t)B * ws * 8 +
+                            (size_t)B * ws * d.M + 1024;
+        const size_t budget = 220 * 1024;
+        uint32_t group = c.group, stages = tuning().lik_stages ? tuning().lik_stages : 8;
+        auto total = [&](uint32_t st, uint32_t g) { return 2 * B * tile + st * g * kstep + 2 * st * 8 + misc; };
+        while (stages > 2 && total(stages, group) > budget) --stages;
+        if (total(stages, group) > budget) continue;
+        p->B = B;
+        p->stages = stages;
+        p->group = group;
+        p->smem = std::max<size_t>(total(stages, group), 116 * 1024);   // one CTA per SM (it takes all TMEM)
+        return true;
+    }
+    return false;
+}
+
 int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T, const float* bias,
                          const uint32_t* list, uint32_t nlist, float* Lk, bool lazy, cudaStream_t st,
                          uint64_t* n_fix_out)
@@ -977,10 +1451,26 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
         FBP_CUDA(cudaMemsetAsync(P.wflag, 0, (size_t)d.nw * d.M, st));
     }
     FBP_CUDA(cudaMemsetAsync(&w.status()->n_fix, 0, 4, st));
-    FBP_CUDA(allow_max_dyn_smem(lik_tc_kernel));
-    const uint32_t grid = (uint32_t)((items + c.ntiles - 1) / c.ntiles);
+    PersistConfig pc;
     count_launch(2);
-    {
+    if (lazy && persist_config(d, c, &pc)) {
+        // the pursuit's passes: persistent CTAs over batches of tiles
+        PersistParams Q;
+        Q.P = P;
+        Q.P.ntiles = pc.B;
+        Q.P.stages = pc.stages;
+        Q.P.group = pc.group;
+        Q.nbatches = (uint32_t)((items + pc.B - 1) / pc.B);
+        int dev = 0, sms = 148;
+        FBP_CUDA(cudaGetDevice(&dev));
+        FBP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        FBP_CUDA(allow_max_dyn_smem(lik_tc_persist_kernel));
+        const uint32_t grid = std::min<uint32_t>(Q.nbatches, (uint32_t)sms);
+        KScope ks(&fbp_chunk_stats::ms_lik_tc, st);
+        lik_tc_persist_kernel<<<grid, kThreads, pc.smem, st>>>(Q);
+    } else {
+        FBP_CUDA(allow_max_dyn_smem(lik_tc_kernel));
+        const uint32_t grid = (uint32_t)((items + c.ntiles - 1) / c.ntiles);
         KScope ks(&fbp_chunk_stats::ms_lik_tc, st);
         lik_tc_kernel<<<grid, kThreads, c.smem, st>>>(P);
     }
