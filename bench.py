@@ -236,7 +236,7 @@ def main():
     bd = torch.from_numpy(bias).to(dev)
     thd = torch.from_numpy(theta).to(dev)
     d = _native.dims(C, N, M, W, S)
-    cap = 4 * (N // W + 1) + 1024
+    cap = 16 * (N // W + 1) + 1024   # every pass adds at most one spike per window; dense probes need several passes
     idx = torch.empty(cap, dtype=torch.int32, device=dev)
     lab = torch.empty(cap, dtype=torch.int32, device=dev)
     P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731

@@ -198,6 +198,260 @@ __device__ float exact_likelihood(const Dims& d, const float* __restrict__ V, co
     return acc;
 }
 
+
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float (&v)[4])
+{
+    uint32_t r[4];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory state of a likelihood CTA's epilogue for its current tiles.
+// Queued runs: t << 14 | tile << 11 | row << 4 | mask (4 consecutive rows).
+struct Epi {
+    const uint32_t* t_s0;    // [tiles] first sample
+    const uint32_t* t_rows;  // [tiles] rows in use
+    const uint32_t* t_w0;    // [tiles] first window
+    const float* sbias;      // [M]
+    const float* bnd;        // [tiles][M] error bound of the estimates
+    int* s_mlb;              // [tiles][wslots] largest lower bound (float bits)
+    uint32_t* s_pos;         // [tiles][wslots] a positive value seen
+    unsigned long long* s_key;   // [tiles][wslots] window maximum key
+    uint8_t* s_inex;         // [tiles][wslots][M] row holds estimates
+    uint32_t* fq;            // [kFixCap]
+    uint32_t* nfq;
+    uint32_t wslots;
+};
+
+// Queueing of the warp's flagged samples of one template (ballot m != 0), out of
+// line: runs of 4 consecutive rows, one entry per non-empty nibble, into the
+// CTA's list, else the global queue, else computed right here.  Returns the
+// sample's exact value if computed here (and sets *here), else `out`.
+__device__ __noinline__ float queue_runs(const Dims d, uint32_t m, bool need, uint32_t t, uint32_t i, uint32_t row,
+                                         uint32_t s, float b, float out, bool* here, uint32_t* fq, uint32_t* nfq,
+                                         DevStatus* status, unsigned long long* fix, uint32_t fix_cap,
+                                         const float* V, const float* T, const float* tnorm)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t nz = 0;   // bit k: nibble k non-empty
+#pragma unroll
+    for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const uint32_t k = lane >> 2;
+    const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
+    const uint32_t nib = (m >> (4 * k)) & 0xFu;
+    const bool local = nib && slot < kFixCap;
+    if ((lane & 3u) == 0 && local) fq[slot] = (t << 14) | (i << 11) | (row << 4) | nib;
+    const bool glob = nib && !local;
+    uint32_t g = 0;
+    if (glob && (lane & 3u) == 0) {
+        g = atomicAdd(&status->n_fix, 1u);
+        if (g < fix_cap) fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | s;
+    }
+    g = __shfl_sync(0xffffffffu, g, lane & ~3u);   // all lanes: the run's first lane holds g
+    const bool queued = local || (glob && g < fix_cap);
+    if (need && !queued) {
+        *here = true;
+        return exact_likelihood(d, V, T, b, t, s, tnorm);
+    }
+    return out;
+}
+
+__device__ __forceinline__ float enqueue(const TcParams& P, const Epi& E, bool need, uint32_t t, uint32_t i,
+                                         uint32_t row, uint32_t s, float b, float out, bool* here)
+{
+    *here = false;
+    const uint32_t m = __ballot_sync(0xffffffffu, need);
+    if (m == 0u) return out;
+    return queue_runs(P.d, m, need, t, i, row, s, b, out, here, E.fq, E.nfq, P.status, P.fix, P.fix_cap, P.V, P.T,
+                      P.tnorm);
+}
+
+// an exact positive value v at (t, s) of tile i: the window's maximum key and positive flag
+__device__ __forceinline__ void note_exact(const Dims& d, const Epi& E, float v, uint32_t t, uint32_t i, uint32_t s)
+{
+    if (!(v > 0.f)) return;
+    const uint32_t w = s / d.W, slot = i * E.wslots + (w - E.t_w0[i]);
+    atomicMax(&E.s_key[slot], window_key(v, t, s - w * d.W));
+    E.s_pos[slot] = 1u;
+}
+
+// Pass 1 of the epilogue over `ntiles` tiles (TMEM columns tbase + i * Np, this
+// thread's row): estimates stored; samples of uncertain sign (lazy) or that can
+// be positive (not lazy) queued; the window slots' largest lower bounds.
+__device__ __forceinline__ void epi_pass1(const TcParams& P, const Epi& E, uint32_t tbase, uint32_t ntiles,
+                                          uint32_t row, bool lazy)
+{
+    const Dims& d = P.d;
+    for (uint32_t i = 0; i < ntiles; ++i) {
+        const uint32_t s = E.t_s0[i] + row;
+        const bool valid = row < E.t_rows[i];
+        const bool live = valid && (uint64_t)s + d.W < d.N;
+        const uint32_t wslot = valid ? i * E.wslots + (s / d.W - E.t_w0[i]) : 0u;
+#pragma unroll 1
+        for (uint32_t t0 = 0; t0 < d.M; t0 += 4) {
+            float v[4];
+            tmem_ld4(tbase + i * P.Np + t0, v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t t = t0 + e;
+                if (t >= d.M) break;   // the same for every lane
+                const float b = E.sbias[t];
+                const float est = v[e] + b;
+                const float bd = E.bnd[i * d.M + t];
+                const bool certain = lazy && live && est - bd > 0.f;
+                const bool need = live && !(est + bd <= 0.f) && !certain;
+                if (certain) {
+                    atomicMax(&E.s_mlb[wslot], __float_as_int(est - bd));
+                    E.s_pos[wslot] = 1u;
+                }
+                bool here = false;
+                const float out = enqueue(P, E, need, t, i, row, s, b, live ? est : 0.f, &here);
+                if (here && lazy) note_exact(d, E, out, t, i, s);
+                if (valid) P.L[(uint64_t)t * d.N + s] = out;
+            }
+        }
+    }
+}
+
+// Pass 2 (lazy): contenders for each window slot's maximum (upper bound reaching
+// its largest lower bound) are queued; the other certainly positive samples keep
+// their estimate and flag their (window, template) row.
+__device__ __forceinline__ void epi_pass2(const TcParams& P, const Epi& E, uint32_t tbase, uint32_t ntiles,
+                                          uint32_t row)
+{
+    const Dims& d = P.d;
+    for (uint32_t i = 0; i < ntiles; ++i) {
+        const uint32_t s = E.t_s0[i] + row;
+        const bool valid = row < E.t_rows[i];
+        const bool live = valid && (uint64_t)s + d.W < d.N;
+        const uint32_t wslot = valid ? i * E.wslots + (s / d.W - E.t_w0[i]) : 0u;
+        const float mlb = __int_as_float(E.s_mlb[wslot]);
+#pragma unroll 1
+        for (uint32_t t0 = 0; t0 < d.M; t0 += 4) {
+            float v[4];
+            tmem_ld4(tbase + i * P.Np + t0, v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t t = t0 + e;
+                if (t >= d.M) break;
+                const float b = E.sbias[t];
+                const float est = v[e] + b;
+                const float bd = E.bnd[i * d.M + t];
+                const bool certain = live && est - bd > 0.f;
+                const bool contender = certain && est + bd >= mlb;
+                bool here = false;
+                const float out = enqueue(P, E, contender, t, i, row, s, b, est, &here);
+                if (here) {
+                    note_exact(d, E, out, t, i, s);
+                    P.L[(uint64_t)t * d.N + s] = out;
+                }
+                if (certain && !contender) E.s_inex[wslot * d.M + t] = 1;
+            }
+        }
+    }
+}
+
+// Exact recomputation of the queued runs, one warp per run (warps w0, w0 + ws,
+// ...): lanes 0..3 carry the run's four samples' sums, each adding its products
+// one at a time in the reference order (channel-major, taps ascending), over the
+// template's non-zero channels (an all-zero channel adds exact zeros); the
+// template row of the next such channel is loaded while the current one is
+// summed and staged in the warp's shared scratch (2 x 128 floats).  Vt: the
+// strips transposed to channel-major rows (channel c of tile i at (i Cp + c) R8).
+__device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, const float* Vt, uint32_t nq,
+                                               uint32_t w0, uint32_t wstride, float* scratch, bool lazy)
+{
+    const Dims& d = P.d;
+    const uint32_t lane = threadIdx.x & 31, W = d.W, Wp = (W + 3) & ~3u, Cp = P.Cq * 4;
+    float* tw = scratch;   // this warp's [2][128]
+    for (uint32_t qi = w0; qi < nq; qi += wstride) {
+        const uint32_t e = E.fq[qi];
+        const uint32_t t = e >> 14, i = (e >> 11) & 7u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
+        const uint32_t k = lane & 3u;   // lanes 4..31 repeat lanes 0..3 and are discarded
+        float acc = E.sbias[t];
+        const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
+        const float* tnr = P.tnorm + (uint64_t)t * d.C;
+        uint32_t c = 0;
+        while (c < d.C && tnr[c] == 0.f) ++c;
+        float tn[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t x = lane + 32u * q;
+            tn[q] = (c < d.C && x < W) ? __ldg(tb + (uint64_t)c * Wp + x) : 0.f;
+        }
+        uint32_t buf = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tw[lane + 32u * q] = tn[q];
+        __syncwarp();
+        while (c < d.C) {
+            uint32_t cn = c + 1;
+            while (cn < d.C && tnr[cn] == 0.f) ++cn;
+            if (cn < d.C) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t x = lane + 32u * q;
+                    tn[q] = x < W ? __ldg(tb + (uint64_t)cn * Wp + x) : 0.f;
+                }
+            }
+            const float* tr = tw + buf * 128u;
+            const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0 + k;
+#pragma unroll 4
+            for (uint32_t j = 0; j < W; ++j) acc = __fadd_rn(acc, __fmul_rn(tr[j], vr[j]));
+            if (cn < d.C) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) tw[(buf ^ 1u) * 128u + lane + 32u * q] = tn[q];
+            }
+            __syncwarp();
+            buf ^= 1u;
+            c = cn;
+        }
+        if (lane < 4 && ((mask >> lane) & 1u)) {
+            const uint32_t sk = E.t_s0[i] + r0 + lane;
+            P.L[(uint64_t)t * d.N + sk] = acc;
+            if (lazy) note_exact(d, E, acc, t, i, sk);
+        }
+        __syncwarp();
+    }
+}
+
+// In-place transposition of `ntq` 4-channel blocks of R8 16-byte rows into
+// channel-major rows of R8 floats, by `nthr` threads (thread index `tid`) that
+// synchronise with `sync()` between reading a block and writing it.
+template <class Sync>
+__device__ __forceinline__ void transpose_strips(unsigned char* A, uint32_t ntq, uint32_t R8, uint32_t tid,
+                                                 uint32_t nthr, Sync sync)
+{
+    const float4* src = reinterpret_cast<const float4*>(A);
+    float* dst = reinterpret_cast<float*>(A);
+    for (uint32_t tq = 0; tq < ntq; ++tq) {
+        float4 vv[2];   // R8 <= 256 rows <= 2 * nthr (nthr >= 128)
+#pragma unroll
+        for (uint32_t k = 0; k < 2; ++k) {
+            const uint32_t r = k * nthr + tid;
+            vv[k] = r < R8 ? src[(size_t)tq * R8 + r] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        sync();
+#pragma unroll
+        for (uint32_t k = 0; k < 2; ++k) {
+            const uint32_t r = k * nthr + tid;
+            if (r >= R8) continue;
+            float* o = dst + (size_t)4 * tq * R8 + r;
+            o[0] = vv[k].x;
+            o[R8] = vv[k].y;
+            o[2 * R8] = vv[k].z;
+            o[3 * R8] = vv[k].w;
+        }
+        sync();
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -349,112 +603,12 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         } else {
             const uint32_t qd = warp & 3;
             const uint32_t row = qd * 32 + lane;
-            // Queue the warp's samples flagged by `need` (template t, tile i) for an
-            // exact recomputation, as runs of 4 consecutive rows (one entry per
-            // non-empty nibble of the ballot): first into this CTA's own list
-            // (recomputed below from the staged strips), then the global queue
-            // (fixup_kernel), else right here.  Returns the sample's exact value if
-            // it was computed here, else `out` unchanged.
-            auto enqueue = [&](bool need, uint32_t t, uint32_t i, uint32_t s, float b, float out, bool& inline_done) {
-                inline_done = false;
-                const uint32_t m = __ballot_sync(0xffffffffu, need);
-                if (m == 0u) return out;
-                uint32_t nz = 0;   // bit k: nibble k non-empty
-#pragma unroll
-                for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
-                uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                const uint32_t k = lane >> 2;
-                const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
-                const uint32_t nib = (m >> (4 * k)) & 0xFu;
-                const bool local = nib && slot < kFixCap;
-                if ((lane & 3u) == 0 && local) fq[slot] = (t << 13) | (i << 11) | (row << 4) | nib;
-                const bool glob = nib && !local;
-                uint32_t g = 0;
-                if (glob && (lane & 3u) == 0) {
-                    g = atomicAdd(&P.status->n_fix, 1u);
-                    if (g < P.fix_cap)
-                        P.fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | s;
-                }
-                g = __shfl_sync(0xffffffffu, g, lane & ~3u);   // all lanes: the run's first lane holds g
-                const bool queued = local || (glob && g < P.fix_cap);
-                if (need && !queued) {
-                    inline_done = true;
-                    return exact_likelihood(d, P.V, P.T, b, t, s, P.tnorm);
-                }
-                return out;
-            };
-            // exact positive value v at (t, s) of tile i: window maximum and sign
-            auto note_exact = [&](float v, uint32_t t, uint32_t i, uint32_t s) {
-                if (!(v > 0.f)) return;
-                const uint32_t w = s / d.W, slot = i * P.wslots + (w - t_w0[i]);
-                atomicMax(&s_key[slot], window_key(v, t, s - w * d.W));
-                s_pos[slot] = 1u;
-            };
-            // pass 1: estimates, bounds, samples of uncertain sign (lazy) or every
-            // sample that can be positive (not lazy)
-            for (uint32_t i = 0; i < P.ntiles; ++i) {
-                const uint32_t s = t_s0[i] + row;
-                const bool valid = row < t_rows[i];
-                const bool live = valid && (uint64_t)s + d.W < d.N;
-                const uint32_t wslot = valid ? i * P.wslots + (s / d.W - t_w0[i]) : 0u;
-                for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
-                    float v[16];
-                    tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const uint32_t t = cg * 16 + e;
-                        if (t >= d.M) continue;   // uniform over the warp
-                        const float b = sbias[t];
-                        const float est = v[e] + b;
-                        const float bd = bnd[i * d.M + t];
-                        const bool certain = P.lazy && live && est - bd > 0.f;
-                        const bool need = live && !(est + bd <= 0.f) && !certain;
-                        if (certain) {
-                            atomicMax(&s_mlb[wslot], __float_as_int(est - bd));
-                            s_pos[wslot] = 1u;
-                        }
-                        bool here = false;
-                        const float out = enqueue(need, t, i, s, b, live ? est : 0.f, here);
-                        if (here && P.lazy) note_exact(out, t, i, s);
-                        if (valid) P.L[(uint64_t)t * d.N + s] = out;
-                    }
-                }
-            }
+            const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
+            const uint32_t tbase = tmem + ((qd * 32) << 16);
+            epi_pass1(P, E, tbase, P.ntiles, row, P.lazy != 0);
             if (P.lazy) {
-                // pass 2: contenders for each window's maximum (upper bound reaching the
-                // window's largest lower bound) are recomputed; the other certainly
-                // positive samples keep their estimate, and their window row is flagged
                 asm volatile("bar.sync 1, 128;" ::: "memory");
-                for (uint32_t i = 0; i < P.ntiles; ++i) {
-                    const uint32_t s = t_s0[i] + row;
-                    const bool valid = row < t_rows[i];
-                    const bool live = valid && (uint64_t)s + d.W < d.N;
-                    const uint32_t wslot = valid ? i * P.wslots + (s / d.W - t_w0[i]) : 0u;
-                    const float mlb = __int_as_float(s_mlb[wslot]);
-                    for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
-                        float v[16];
-                        tmem_ld16(tmem + ((qd * 32) << 16) + i * P.Np + cg * 16, v);
-#pragma unroll
-                        for (int e = 0; e < 16; ++e) {
-                            const uint32_t t = cg * 16 + e;
-                            if (t >= d.M) continue;
-                            const float b = sbias[t];
-                            const float est = v[e] + b;
-                            const float bd = bnd[i * d.M + t];
-                            const bool certain = live && est - bd > 0.f;
-                            const bool contender = certain && est + bd >= mlb;
-                            bool here = false;
-                            const float out = enqueue(contender, t, i, s, b, est, here);
-                            if (here) {
-                                note_exact(out, t, i, s);
-                                P.L[(uint64_t)t * d.N + s] = out;
-                            }
-                            if (certain && !contender) s_inex[wslot * d.M + t] = 1;
-                        }
-                    }
-                }
+                epi_pass2(P, E, tbase, P.ntiles, row);
             }
         }
         tc_fence_before();
@@ -468,106 +622,22 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
     }
-    // exact recomputation of this CTA's queued runs, all warps.  The strips are
-    // transposed in place to channel-major rows (channel c of tile i at
-    // (i Cp + c) R8 floats), so a run reads its voltage with aligned 16-byte
-    // loads: 8 consecutive samples per 4 taps, rows of one epilogue warp's band
-    // landing in distinct banks.
+    // exact recomputation of this CTA's queued runs, all warps, from the strips
+    // transposed in place to channel-major rows; each warp stages template rows in
+    // its share of the (now idle) template ring
     const uint32_t nq = min(*nfq, kFixCap);
     if (threadIdx.x == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
     if (nq == 0 && !P.lazy) return;
-    // the strips were written by bulk copies and read by the MMAs (async proxy)
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    const uint32_t Cp = P.Cq * 4;
+    const uint32_t W = d.W;
     if (nq > 0) {
-        // each 4-channel block of R8 16-byte rows becomes 4 channel rows of R8
-        // floats in the same bytes: one block at a time, read fully, then written
-        constexpr uint32_t kPer = 2;   // R8 <= 256 rows <= kPer * blockDim
-        const float4* src = reinterpret_cast<const float4*>(A);
-        float* dst = reinterpret_cast<float*>(A);
-        for (uint32_t tq = 0; tq < P.ntiles * P.Cq; ++tq) {
-            float4 v[kPer];
-#pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) {
-                const uint32_t row = k * blockDim.x + threadIdx.x;
-                v[k] = row < P.R8 ? src[(size_t)tq * P.R8 + row] : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            __syncthreads();
-#pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) {
-                const uint32_t row = k * blockDim.x + threadIdx.x;
-                if (row >= P.R8) continue;
-                float* o = dst + (size_t)4 * tq * P.R8 + row;
-                o[0] = v[k].x;
-                o[P.R8] = v[k].y;
-                o[2 * P.R8] = v[k].z;
-                o[3 * P.R8] = v[k].w;
-            }
-            __syncthreads();
-        }
+        // the strips were written by bulk copies and read by the MMAs (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        transpose_strips(A, P.ntiles * P.Cq, P.R8, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+        const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
+        recompute_runs(P, E, reinterpret_cast<const float*>(A), nq, warp, blockDim.x >> 5,
+                       reinterpret_cast<float*>(B) + warp * 256u, P.lazy != 0);
     }
-    const uint32_t W = d.W, Wp = (W + 3) & ~3u;
-    const float* Vt = reinterpret_cast<const float*>(A);
-    // One warp per queued run.  Lanes 0..3 carry the run's four samples' sums, each
-    // adding its products one at a time in the reference order (channel-major, taps
-    // ascending); the warp loads each template channel row coalesced -- the next
-    // row while the current one is summed -- and broadcasts tap j by shuffle, so a
-    // run costs about one dependent add per tap rather than a global load per 4 taps.
-    const uint32_t nwarp = blockDim.x >> 5;
-    for (uint32_t qi = warp; qi < nq; qi += nwarp) {
-        const uint32_t e = fq[qi];
-        const uint32_t t = e >> 13, i = (e >> 11) & 3u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
-        const uint32_t k = lane & 3u;   // lanes 4..31 repeat lanes 0..3 and are discarded
-        float acc = sbias[t];
-        const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
-        // template channels that are entirely zero add 0 * v terms: skipped
-        const float* tnr = P.tnorm + (uint64_t)t * d.C;
-        auto next_active = [&](uint32_t c) {
-            while (c < d.C && tnr[c] == 0.f) ++c;
-            return c;
-        };
-        float tv[4], tn[4];
-        uint32_t c = next_active(0);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint32_t x = lane + 32u * q;
-            tn[q] = (c < d.C && x < W) ? __ldg(tb + (uint64_t)c * Wp + x) : 0.f;
-        }
-        while (c < d.C) {
-            const uint32_t cn = next_active(c + 1);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) tv[q] = tn[q];
-            if (cn < d.C) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t x = lane + 32u * q;
-                    tn[q] = x < W ? __ldg(tb + (uint64_t)cn * Wp + x) : 0.f;
-                }
-            }
-            const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0 + k;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-#pragma unroll
-                for (int jj = 0; jj < 32; ++jj) {
-                    const uint32_t j = 32u * q + jj;
-                    if (j < W) {   // the same for every lane
-                        const float tj = __shfl_sync(0xffffffffu, tv[q], jj);
-                        acc = __fadd_rn(acc, __fmul_rn(tj, vr[j]));
-                    }
-                }
-            }
-            c = cn;
-        }
-        if (lane < 4 && ((mask >> lane) & 1u)) {
-            const uint32_t sk = t_s0[i] + r0 + lane;
-            P.L[(uint64_t)t * d.N + sk] = acc;
-            if (P.lazy && acc > 0.f) {
-                const uint32_t w = sk / W, slot = i * P.wslots + (w - t_w0[i]);
-                atomicMax(&s_key[slot], window_key(acc, t, sk - w * W));
-                s_pos[slot] = 1u;
-            }
-        }
-    }
+    __syncthreads();
     if (!P.lazy) return;
     // publish each touched window's maximum key and positive flag: a listed window
     // belongs to this CTA alone (stored); a tile of the whole-chunk pass shares its
@@ -596,11 +666,6 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
     }
 }
 
-// Exact recomputation of the queued runs (reference order, FP32).  An entry
-// is (t << 40) | (mask << 32) | s0: samples s0 + k with bit k of the 4-bit mask
-// set.  A thread carries the four samples' sequential sums side by side: per 4
-// taps one 16-byte template load and 4 voltage loads feed 16 multiply-adds
-// (each sum still adds its products one at a time, in the reference's order).
 // ---------------------------------------------------------------------------
 // Persistent tensor-core likelihood (the pursuit's passes, lazy exactness).
 //
@@ -673,6 +738,8 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
     unsigned long long* s_key = reinterpret_cast<unsigned long long*>(
         (reinterpret_cast<uintptr_t>(s_pos + B * P.wslots) + 7) & ~(uintptr_t)7);
     uint8_t* s_inex = reinterpret_cast<uint8_t*>(s_key + B * P.wslots);   // [B][wslots][M]
+    float* scratch = reinterpret_cast<float*>(
+        (reinterpret_cast<uintptr_t>(s_inex + B * P.wslots * d.M) + 15) & ~(uintptr_t)15);   // [4 warps][256]
 
     const uint32_t ksteps = d.W * (P.Cq / 2);
     const uint32_t ngroups = (ksteps + P.group - 1) / P.group;
@@ -814,102 +881,10 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
             if (!epi_all(mbar_wait(&acc_full[s], use & 1))) { if (et == 0) atomicOr(err, 8u); break; }
             tc_fence_after();
             const uint32_t tbase = tmem + ((qd * 32) << 16) + s * 256u;
-            auto enqueue = [&](bool need, uint32_t t, uint32_t i, uint32_t sm_, float b, float out, bool& here) {
-                here = false;
-                const uint32_t m = __ballot_sync(0xffffffffu, need);
-                if (m == 0u) return out;
-                uint32_t nz = 0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
-                uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                const uint32_t k = lane >> 2;
-                const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
-                const uint32_t nib = (m >> (4 * k)) & 0xFu;
-                const bool local = nib && slot < kFixCap;
-                if ((lane & 3u) == 0 && local) fq[slot] = (t << 14) | (i << 11) | (row << 4) | nib;
-                const bool glob = nib && !local;
-                uint32_t g = 0;
-                if (glob && (lane & 3u) == 0) {
-                    g = atomicAdd(&P.status->n_fix, 1u);
-                    if (g < P.fix_cap)
-                        P.fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | sm_;
-                }
-                g = __shfl_sync(0xffffffffu, g, lane & ~3u);
-                const bool queued = local || (glob && g < P.fix_cap);
-                if (need && !queued) {
-                    here = true;
-                    return exact_likelihood(d, P.V, P.T, b, t, sm_, P.tnorm);
-                }
-                return out;
-            };
-            auto note_exact = [&](float v, uint32_t t, uint32_t i, uint32_t sm_, const uint32_t* w0) {
-                if (!(v > 0.f)) return;
-                const uint32_t w = sm_ / d.W, slot = i * P.wslots + (w - w0[i]);
-                atomicMax(&s_key[slot], window_key(v, t, sm_ - w * d.W));
-                s_pos[slot] = 1u;
-            };
-            // pass 1: estimates, samples of uncertain sign, the window's largest lower bound
-            for (uint32_t i = 0; i < B; ++i) {
-                const uint32_t sm_ = t_s0[i] + row;
-                const bool valid = row < t_rows[i];
-                const bool live = valid && (uint64_t)sm_ + d.W < d.N;
-                const uint32_t wslot = valid ? i * P.wslots + (sm_ / d.W - t_w0[i]) : 0u;
-                for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
-                    float v[16];
-                    tmem_ld16(tbase + i * P.Np + cg * 16, v);
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const uint32_t t = cg * 16 + e;
-                        if (t >= d.M) continue;
-                        const float b = sbias[t];
-                        const float est = v[e] + b;
-                        const float bd = bnd[i * d.M + t];
-                        const bool certain = live && est - bd > 0.f;
-                        const bool need = live && !(est + bd <= 0.f) && !certain;
-                        if (certain) {
-                            atomicMax(&s_mlb[wslot], __float_as_int(est - bd));
-                            s_pos[wslot] = 1u;
-                        }
-                        bool here = false;
-                        const float out = enqueue(need, t, i, sm_, b, live ? est : 0.f, here);
-                        if (here) note_exact(out, t, i, sm_, t_w0);
-                        if (valid) P.L[(uint64_t)t * d.N + sm_] = out;
-                    }
-                }
-            }
+            const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
+            epi_pass1(P, E, tbase, B, row, true);
             asm volatile("bar.sync 1, 128;" ::: "memory");
-            // pass 2: contenders for each window's maximum are recomputed; the other
-            // certainly positive samples keep their estimate, their window row flagged
-            for (uint32_t i = 0; i < B; ++i) {
-                const uint32_t sm_ = t_s0[i] + row;
-                const bool valid = row < t_rows[i];
-                const bool live = valid && (uint64_t)sm_ + d.W < d.N;
-                const uint32_t wslot = valid ? i * P.wslots + (sm_ / d.W - t_w0[i]) : 0u;
-                const float mlb = __int_as_float(s_mlb[wslot]);
-                for (uint32_t cg = 0; cg < P.Np / 16; ++cg) {
-                    float v[16];
-                    tmem_ld16(tbase + i * P.Np + cg * 16, v);
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const uint32_t t = cg * 16 + e;
-                        if (t >= d.M) continue;
-                        const float b = sbias[t];
-                        const float est = v[e] + b;
-                        const float bd = bnd[i * d.M + t];
-                        const bool certain = live && est - bd > 0.f;
-                        const bool contender = certain && est + bd >= mlb;
-                        bool here = false;
-                        const float out = enqueue(contender, t, i, sm_, b, est, here);
-                        if (here) {
-                            note_exact(out, t, i, sm_, t_w0);
-                            P.L[(uint64_t)t * d.N + sm_] = out;
-                        }
-                        if (certain && !contender) s_inex[wslot * d.M + t] = 1;
-                    }
-                }
-            }
+            epi_pass2(P, E, tbase, B, row);
             // TMEM buffer s read: the MMAs of batch it+2 may use it
             tc_fence_before();
             asm volatile("bar.sync 1, 128;" ::: "memory");
@@ -918,88 +893,13 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
             // place to channel-major rows (the MMAs of this batch are complete)
             const uint32_t nq = min(*nfq, kFixCap);
             if (et == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
-            const uint32_t Cp = P.Cq * 4;
             if (nq > 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                constexpr uint32_t kPer = 2;   // R8 <= 256 rows <= kPer * 128
-                const float4* src = reinterpret_cast<const float4*>(Ab);
-                float* dst = reinterpret_cast<float*>(Ab);
-                for (uint32_t tq = 0; tq < B * P.Cq; ++tq) {
-                    float4 vv[kPer];
-#pragma unroll
-                    for (uint32_t k = 0; k < kPer; ++k) {
-                        const uint32_t r = k * 128 + et;
-                        vv[k] = r < P.R8 ? src[(size_t)tq * P.R8 + r] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
-                    asm volatile("bar.sync 1, 128;" ::: "memory");
-#pragma unroll
-                    for (uint32_t k = 0; k < kPer; ++k) {
-                        const uint32_t r = k * 128 + et;
-                        if (r >= P.R8) continue;
-                        float* o = dst + (size_t)4 * tq * P.R8 + r;
-                        o[0] = vv[k].x;
-                        o[P.R8] = vv[k].y;
-                        o[2 * P.R8] = vv[k].z;
-                        o[3 * P.R8] = vv[k].w;
-                    }
-                    asm volatile("bar.sync 1, 128;" ::: "memory");
-                }
+                transpose_strips(Ab, B * P.Cq, P.R8, et, 128u, [] { asm volatile("bar.sync 1, 128;" ::: "memory"); });
+                const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
+                recompute_runs(P, E, reinterpret_cast<const float*>(Ab), nq, ew, 4u, scratch + ew * 256u, true);
             }
-            const uint32_t W = d.W, Wp = (W + 3) & ~3u;
-            const float* Vt = reinterpret_cast<const float*>(Ab);
-            for (uint32_t qi = ew; qi < nq; qi += 4) {
-                const uint32_t e = fq[qi];
-                const uint32_t t = e >> 14, i = (e >> 11) & 7u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
-                const uint32_t k = lane & 3u;
-                float acc = sbias[t];
-                const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
-                const float* tnr = P.tnorm + (uint64_t)t * d.C;
-                auto next_active = [&](uint32_t c) {
-                    while (c < d.C && tnr[c] == 0.f) ++c;
-                    return c;
-                };
-                float tv[4], tn[4];
-                uint32_t c = next_active(0);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t x = lane + 32u * q;
-                    tn[q] = (c < d.C && x < W) ? __ldg(tb + (uint64_t)c * Wp + x) : 0.f;
-                }
-                while (c < d.C) {
-                    const uint32_t cn = next_active(c + 1);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) tv[q] = tn[q];
-                    if (cn < d.C) {
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const uint32_t x = lane + 32u * q;
-                            tn[q] = x < W ? __ldg(tb + (uint64_t)cn * Wp + x) : 0.f;
-                        }
-                    }
-                    const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0 + k;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-#pragma unroll
-                        for (int jj = 0; jj < 32; ++jj) {
-                            const uint32_t j = 32u * q + jj;
-                            if (j < W) {
-                                const float tj = __shfl_sync(0xffffffffu, tv[q], jj);
-                                acc = __fadd_rn(acc, __fmul_rn(tj, vr[j]));
-                            }
-                        }
-                    }
-                    c = cn;
-                }
-                if (lane < 4 && ((mask >> lane) & 1u)) {
-                    const uint32_t sk = t_s0[i] + r0 + lane;
-                    P.L[(uint64_t)t * d.N + sk] = acc;
-                    if (acc > 0.f) {
-                        const uint32_t w = sk / W, slot = i * P.wslots + (w - t_w0[i]);
-                        atomicMax(&s_key[slot], window_key(acc, t, sk - w * W));
-                        s_pos[slot] = 1u;
-                    }
-                }
-            }
+            const uint32_t W = d.W;
             asm volatile("bar.sync 1, 128;" ::: "memory");
             // publish the batch's window maxima, positive flags and estimate flags
             for (uint32_t e = et; e < B * P.wslots; e += 128) {
@@ -1053,6 +953,11 @@ __device__ __forceinline__ void note_window(const Dims& d, unsigned long long* w
     wpos[w] = 1;
 }
 
+// Exact recomputation of the queued runs (reference order, FP32).  An entry
+// is (t << 40) | (mask << 32) | s0: samples s0 + k with bit k of the 4-bit mask
+// set.  A thread carries the four samples' sequential sums side by side: per 4
+// taps one 16-byte template load and 4 voltage loads feed 16 multiply-adds
+// (each sum still adds its products one at a time, in the reference's order).
 __global__ void fixup_kernel(Dims d, const float* __restrict__ V, const float* __restrict__ T,
                              const float* __restrict__ Tp, const float* __restrict__ bias,
                              const unsigned long long* __restrict__ fix, uint32_t cap, const DevStatus* status,
@@ -1285,6 +1190,8 @@ bool tc_config(const Dims& d, TcConfig* c)
         c->group = tu.lik_group ? tu.lik_group : (uint32_t)std::max<size_t>(1, (6 * 1024) / kstep);
         c->stages = tu.lik_stages ? tu.lik_stages : 3;
         while (c->group > 1 && strips + c->stages * c->group * kstep > 160 * 1024) c->group >>= 1;
+        // after the MMAs the ring is the exact recomputation's scratch: 6 warps x 1 KB
+        while (c->stages * c->group * kstep < 6 * 1024 + 256) ++c->group;
         const size_t misc = 8 + c->ntiles * 8 + (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 +
                             (size_t)kFixCap * 4 + 4 + (size_t)c->ntiles * 4 + (size_t)c->ntiles * win_slots(d.W) * (16 + d.M) + 8 +
                             1024;
@@ -1385,7 +1292,7 @@ bool persist_config(const Dims& d, const TcConfig& c, PersistConfig* p)
     for (; B >= 2; --B) {
         const size_t misc = (9 + 0) * 8 + 8 + 6 * B * 4 + (size_t)B * (d.C + d.M) * 4 + (size_t)d.M * 4 +
                             (size_t)kFixCap * 4 + 4 + (size_t)B * ws * 8 + 8 + (size_t)B * ws * 8 +
-                            (size_t)B * ws * d.M + 1024;
+                            (size_t)B * ws * d.M + 16 + 4 * 256 * 4 + 1024;
         const size_t budget = 220 * 1024;
         uint32_t group = c.group, stages = tuning().lik_stages ? tuning().lik_stages : 8;
         auto total = [&](uint32_t st, uint32_t g) { return 2 * B * tile + st * g * kstep + 2 * st * 8 + misc; };
