@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define FBP_ABI_VERSION 3
+#define FBP_ABI_VERSION 4
 
 typedef enum fbp_status {
     FBP_OK = 0,
@@ -97,6 +97,7 @@ typedef struct fbp_tuning {
     uint32_t lik_group;    /* (tap, channel pair) steps of templates per staged copy */
     uint32_t lik_stages;   /* staged template copies in flight: 2 to 8 */
     uint32_t pc_group;     /* templates per partial-correlation CTA: 1, 2, 4 or 8 */
+    uint32_t lik_epi;      /* epilogue warpgroups of the persistent likelihood CTA: 1 to 4 */
 } fbp_tuning;
 
 /* Set the calling thread's launch shapes for its later calls (NULL: the

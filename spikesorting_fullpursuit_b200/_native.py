@@ -31,7 +31,7 @@ EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_purs
            "fbp_residual_covariance", "fbp_set_tuning")
 NOALLOC_MAX_SPIKES = 65536
 PASS_RING = 64
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 
 class FbpDims(ctypes.Structure):
@@ -66,7 +66,7 @@ class FbpChunkStats(ctypes.Structure):
 
 class FbpTuning(ctypes.Structure):
     _fields_ = [("lik_tiles", ctypes.c_uint32), ("lik_group", ctypes.c_uint32), ("lik_stages", ctypes.c_uint32),
-                ("pc_group", ctypes.c_uint32)]
+                ("pc_group", ctypes.c_uint32), ("lik_epi", ctypes.c_uint32)]
 
 
 class FbpError(RuntimeError):

@@ -25,7 +25,7 @@ import numpy as np
 from . import _native
 
 _LOCK = threading.Lock()
-FIELDS = ("lik_tiles", "lik_group", "lik_stages", "pc_group")
+FIELDS = ("lik_tiles", "lik_group", "lik_stages", "pc_group", "lik_epi")
 
 
 def cache_path():
@@ -86,13 +86,16 @@ def _time(torch, fn, reps=3):
 
 
 def lik_candidates(M):
+    """Likelihood launch shapes to measure: the persistent kernel (lik_tiles 0)
+    with 1 to 4 epilogue warpgroups, then per-CTA tile counts."""
     Np = (M + 15) // 16 * 16
+    out = [{"lik_tiles": 0, "lik_epi": e, "lik_stages": st, "lik_group": 0, "pc_group": 0}
+           for e in (2, 3, 1, 4) for st in (0, 4)]
     tiles = tuple(k for k in (2, 4, 1) if k * Np <= 512)
-    out = []
     for lt in tiles:
         for st in (0, 4, 6):
             for g in (0, 2, 8):
-                out.append({"lik_tiles": lt, "lik_stages": st, "lik_group": g, "pc_group": 0})
+                out.append({"lik_tiles": lt, "lik_stages": st, "lik_group": g, "pc_group": 0, "lik_epi": 0})
     return out
 
 

@@ -199,7 +199,7 @@ extern "C" int fbp_set_tuning(const fbp_tuning* t)
         tuning() = fbp_tuning{};
         return FBP_OK;
     }
-    if (t->lik_tiles > 4 || (t->lik_stages != 0 && (t->lik_stages < 2 || t->lik_stages > 8)) ||
+    if (t->lik_tiles > 4 || t->lik_epi > 4 || (t->lik_stages != 0 && (t->lik_stages < 2 || t->lik_stages > 8)) ||
         (t->pc_group != 0 && t->pc_group != 1 && t->pc_group != 2 && t->pc_group != 4 && t->pc_group != 8) ||
         t->lik_group > 64)
         return fail(FBP_E_ARG, "tuning value out of range");
@@ -213,12 +213,6 @@ extern "C" size_t fbp_workspace_bytes(const fbp_dims* dims, uint32_t flags)
     if (!make_layout(dims, flags, &L)) return 0;
     return L.bytes;
 }
-
-#define FBP_TRY(expr)                 \
-    do {                              \
-        int rc_ = (expr);             \
-        if (rc_ != FBP_OK) return rc_; \
-    } while (0)
 
 extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* voltage,
                                 const float* templates, const float* bias, const float* theta,

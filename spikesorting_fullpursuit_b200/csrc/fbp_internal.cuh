@@ -24,6 +24,12 @@ int fail(int status, const std::string& msg);
             return ::fbp::fail(FBP_E_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+#define FBP_TRY(expr)                  \
+    do {                               \
+        int rc_ = (expr);              \
+        if (rc_ != FBP_OK) return rc_; \
+    } while (0)
+
 // Every launcher sets a kernel's dynamic shared-memory limit to the largest the
 // device allows for that kernel (the block opt-in maximum less the kernel's
 // static shared memory): the attribute belongs to the kernel in the whole

@@ -481,31 +481,46 @@ __global__ void __launch_bounds__(kOvThreads) overlap_plain_kernel(
 // flagged window, from the winner key.
 // ---------------------------------------------------------------------------
 // Exact likelihood of (t, s) in the reference order (compute_maximum_likelihood,
-// binary_pursuit.cl:216-252) from the current voltage.
-__device__ float exact_lik(const Dims& d, const float* __restrict__ V, const float* __restrict__ T, float b,
-                           uint32_t t, uint32_t s, const float* __restrict__ tnorm)
+// binary_pursuit.cl:216-252) from the current voltage, by a whole warp: each
+// lane forms the products of 32 taps at a time (each product rounds the same
+// wherever it is formed), and every lane adds them in tap order, so all lanes
+// end with the reference's sum.  Channels where the template is entirely zero
+// add 0 * v terms in the reference, which leave a nonzero sum unchanged.
+__device__ float warp_exact_lik(const Dims& d, const float* __restrict__ V, const float* __restrict__ T, float b,
+                                uint32_t t, uint32_t s, const float* __restrict__ tnorm)
 {
+    const uint32_t lane = threadIdx.x & 31;
     float acc = b;
     for (uint32_t c = 0; c < d.C; ++c) {
-        if (tnorm[(uint64_t)t * d.C + c] == 0.f) continue;   // an all-zero template channel adds 0
+        if (tnorm[(uint64_t)t * d.C + c] == 0.f) continue;
         const float* tr = T + ((uint64_t)t * d.C + c) * d.W;
         const float* vr = V + (uint64_t)c * d.N + s;
-        for (uint32_t j = 0; j < d.W; ++j) acc = fadd(acc, fmul(tr[j], vr[j]));
+        for (uint32_t j0 = 0; j0 < d.W; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            const float p = j < d.W ? fmul(__ldg(tr + j), vr[j]) : 0.f;
+            const uint32_t n = d.W - j0 < 32u ? d.W - j0 : 32u;
+#pragma unroll 8
+            for (uint32_t k = 0; k < n; ++k) acc = fadd(acc, __shfl_sync(0xffffffffu, p, k));
+        }
     }
     return acc;
 }
 
 // L[t][s], made exact where the tensor-core likelihood may have left an estimate
 // (a positive value in a flagged window row; the window's voltage is unchanged
-// since it was computed, so the current voltage gives the exact value).
-__device__ __forceinline__ float lik_value(const Dims& d, const float* __restrict__ L, const LazyRef& z, uint32_t t,
-                                           uint32_t s)
+// since it was computed, so the current voltage gives the exact value).  Called
+// by a whole warp with the same (t, s) on every lane.
+__device__ __forceinline__ float warp_lik_value(const Dims& d, const float* __restrict__ L, const LazyRef& z,
+                                                uint32_t t, uint32_t s)
 {
     const float v = L[(uint64_t)t * d.N + s];
-    if (z.wflag != nullptr && v > 0.f && z.wflag[(uint64_t)(s / d.W) * d.M + t]) return exact_lik(d, z.V, z.T, z.bias[t], t, s, z.tnorm);
+    if (z.wflag != nullptr && v > 0.f && z.wflag[(uint64_t)(s / d.W) * d.M + t])
+        return warp_exact_lik(d, z.V, z.T, z.bias[t], t, s, z.tnorm);
     return v;
 }
 
+// One warp per flagged window (every lane evaluates the same decisions; lane 0
+// writes them).
 __global__ void parse_kernel(Dims d, const float* __restrict__ L, const float* __restrict__ theta,
                              const uint32_t* __restrict__ flag, const DevStatus* status,
                              const unsigned long long* __restrict__ keys, float* best_lik,
@@ -515,26 +530,35 @@ __global__ void parse_kernel(Dims d, const float* __restrict__ L, const float* _
     const uint32_t nflag = status->n_flag;
     const uint64_t S2 = 2ull * d.S + 1;
     const uint64_t items = S2 * S2 * d.M;
+    const bool lead = (threadIdx.x & 31) == 0;
     uint32_t lbits = 0;
     while ((1u << lbits) < d.WG) ++lbits;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nflag; k += gridDim.x * blockDim.x) {
+    const uint32_t wpb = blockDim.x >> 5;
+    for (uint32_t k = blockIdx.x * wpb + (threadIdx.x >> 5); k < nflag; k += gridDim.x * wpb) {
         const uint32_t id = flag[k];
         const float seed = best_lik[id];
         const unsigned long long key = keys[k];
         const bool have = key != 0ull;
         const float gv = have ? __uint_as_float((uint32_t)(key >> 32)) : 0.f;
-        if (!have || gv <= seed || gv <= 0.f) { orech[id] = 0; continue; }
+        if (!have || gv <= seed || gv <= 0.f) {
+            if (lead) orech[id] = 0;
+            continue;
+        }
         const uint32_t prio = 0xFFFFFFFFu - (uint32_t)(key & 0xFFFFFFFFull);
         const uint32_t g = prio / d.WG, lb = prio % d.WG;
         const uint32_t l = lbits ? (__brev(lb) >> (32 - lbits)) : 0u;
         const uint64_t r = (uint64_t)g * d.WG + l;
-        if (r >= items) { orech[id] = 0; continue; }
+        if (r >= items) {
+            if (lead) orech[id] = 0;
+            continue;
+        }
         const uint32_t f = best_lab[id], p = best_idx[id];
         const uint32_t t = (uint32_t)(r % d.M);
         const uint64_t a = (r / d.M) % S2, b = (r / (S2 * d.M)) % S2;
         const uint32_t afi = (uint32_t)(p + a - d.S), asi = (uint32_t)(p + b - d.S);
-        const float l1 = lik_value(d, L, z, f, afi);
-        const float l2 = lik_value(d, L, z, t, asi);
+        const float l1 = warp_lik_value(d, L, z, f, afi);
+        const float l2 = warp_lik_value(d, L, z, t, asi);
+        if (!lead) continue;
         if (gv < l1 || gv < l2) { orech[id] = 0; continue; }
         if (l1 <= 0.f || l2 <= 0.f) { orech[id] = 0; continue; }
         if (l1 >= l2 && l1 > theta[f]) { best_lik[id] = l1; ov_lab[id] = f; ov_idx[id] = afi; }
@@ -979,13 +1003,14 @@ int launch_parse_reassign(const Dims& d, const Work& w, const float* theta, uint
 {
     if (nflag_max == 0) return FBP_OK;
     const uint32_t g = grid_for(nflag_max, 256);
+    const uint32_t gw = grid_for(nflag_max, 8);   // parse: one warp per window
     LazyRef z{nullptr, nullptr, V, T, bias};
     if (lazy) {
         z.wflag = w.at<uint8_t>(w.lay->off_wflag);
         z.tnorm = w.at<float>(w.lay->off_tnorm);
     }
     count_launch(5);
-    parse_kernel<<<g, 256, 0, st>>>(d, w.L(), theta, w.flag(), w.status(), w.keys(), w.best_lik(),
+    parse_kernel<<<gw, 256, 0, st>>>(d, w.L(), theta, w.flag(), w.status(), w.keys(), w.best_lik(),
                                     w.best_lab(), w.best_idx(), w.orech(), w.ov_idx(), w.ov_lab(), z);
     reassign_resolve_kernel<<<g, 256, 0, st>>>(d, w.flag(), w.status(), w.orech(), w.ov_idx(), w.orech_fin());
     reassign_apply_kernel<<<g, 256, 0, st>>>(d, w.flag(), w.status(), w.orech(), w.orech_fin(), w.best_idx(),

@@ -42,7 +42,7 @@ namespace {
 constexpr int kTile = 128;         // samples per UMMA tile (M)
 constexpr int kThreads = 192;
 constexpr uint64_t kWaitNs = 250ull * 1000ull * 1000ull;   // longest mbarrier wait (global timer)
-constexpr uint32_t kFixCap = 1024;   // runs recomputed in the CTA itself; more go to the global queue
+constexpr uint32_t kFixCap = 512;   // queued 32-row entries recomputed in the CTA itself; more go to the global queue
 // windows one tile of 128 consecutive samples can touch
 __host__ __device__ __forceinline__ uint32_t win_slots(uint32_t W) { return (kTile + W - 1) / W + 1; }
 
@@ -132,19 +132,6 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar)
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 struct TcParams {
     Dims d;
     const float* V;       // [C][N] (exact recomputation)
@@ -199,19 +186,25 @@ __device__ float exact_likelihood(const Dims& d, const float* __restrict__ V, co
 }
 
 
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float (&v)[4])
+// TMEM -> registers: 4 consecutive accumulator columns of the warp's 32 lanes.
+// The wait is a separate statement that names the destination registers, so no
+// use of them is scheduled before it and a load can be in flight while the
+// previous group is processed (no function call may come between the two).
+__device__ __forceinline__ void tmem_ld4_issue(uint32_t taddr, uint32_t (&r)[4])
 {
-    uint32_t r[4];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
                  : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait4(uint32_t (&r)[4])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])::"memory");
 }
 
 // Shared-memory state of a likelihood CTA's epilogue for its current tiles.
-// Queued runs: t << 14 | tile << 11 | row << 4 | mask (4 consecutive rows).
+// Queued runs: mask << 32 | t << 5 | tile << 2 | quarter -- rows 32 quarter + k of
+// the tile for the set bits k of the mask.
 struct Epi {
     const uint32_t* t_s0;    // [tiles] first sample
     const uint32_t* t_rows;  // [tiles] rows in use
@@ -222,41 +215,36 @@ struct Epi {
     uint32_t* s_pos;         // [tiles][wslots] a positive value seen
     unsigned long long* s_key;   // [tiles][wslots] window maximum key
     uint8_t* s_inex;         // [tiles][wslots][M] row holds estimates
-    uint32_t* fq;            // [kFixCap]
+    unsigned long long* fq;  // [kFixCap]
     uint32_t* nfq;
     uint32_t wslots;
 };
 
 // Queueing of the warp's flagged samples of one template (ballot m != 0), out of
-// line: runs of 4 consecutive rows, one entry per non-empty nibble, into the
-// CTA's list, else the global queue, else computed right here.  Returns the
-// sample's exact value if computed here (and sets *here), else `out`.
+// line: one entry for the warp's 32 rows in the CTA's list; when that is full,
+// runs of 4 rows in the global queue; when that is full too, computed right here.
+// Returns the sample's exact value if computed here (and sets *here), else `out`.
 __device__ __noinline__ float queue_runs(const Dims d, uint32_t m, bool need, uint32_t t, uint32_t i, uint32_t row,
-                                         uint32_t s, float b, float out, bool* here, uint32_t* fq, uint32_t* nfq,
-                                         DevStatus* status, unsigned long long* fix, uint32_t fix_cap,
+                                         uint32_t s, float b, float out, bool* here, unsigned long long* fq,
+                                         uint32_t* nfq, DevStatus* status, unsigned long long* fix, uint32_t fix_cap,
                                          const float* V, const float* T, const float* tnorm)
 {
     const uint32_t lane = threadIdx.x & 31;
-    uint32_t nz = 0;   // bit k: nibble k non-empty
-#pragma unroll
-    for (int k = 0; k < 8; ++k) nz |= ((m >> (4 * k)) & 0xFu) ? (1u << k) : 0u;
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(nfq, (uint32_t)__popc(nz));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    const uint32_t k = lane >> 2;
-    const uint32_t slot = base + __popc(nz & ((1u << k) - 1u));
-    const uint32_t nib = (m >> (4 * k)) & 0xFu;
-    const bool local = nib && slot < kFixCap;
-    if ((lane & 3u) == 0 && local) fq[slot] = (t << 14) | (i << 11) | (row << 4) | nib;
-    const bool glob = nib && !local;
+    uint32_t slot = 0;
+    if (lane == 0) slot = atomicAdd(nfq, 1u);
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    if (slot < kFixCap) {
+        if (lane == 0) fq[slot] = ((unsigned long long)m << 32) | (t << 5) | (i << 2) | (row >> 5);
+        return out;
+    }
+    const uint32_t nib = (m >> (4 * (lane >> 2))) & 0xFu;
     uint32_t g = 0;
-    if (glob && (lane & 3u) == 0) {
+    if (nib && (lane & 3u) == 0) {
         g = atomicAdd(&status->n_fix, 1u);
         if (g < fix_cap) fix[g] = ((unsigned long long)t << 40) | ((unsigned long long)nib << 32) | s;
     }
     g = __shfl_sync(0xffffffffu, g, lane & ~3u);   // all lanes: the run's first lane holds g
-    const bool queued = local || (glob && g < fix_cap);
-    if (need && !queued) {
+    if (need && g >= fix_cap) {
         *here = true;
         return exact_likelihood(d, V, T, b, t, s, tnorm);
     }
@@ -282,11 +270,74 @@ __device__ __forceinline__ void note_exact(const Dims& d, const Epi& E, float v,
     E.s_pos[slot] = 1u;
 }
 
+// The same for the exact values of the lanes with `has`, one atomic per window
+// slot the warp's rows meet.
+__device__ __forceinline__ void warp_note_exact(const Dims& d, const Epi& E, bool has, float v, uint32_t t,
+                                                uint32_t i, uint32_t s)
+{
+    const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31;
+    has = has && v > 0.f;
+    uint32_t pend = __ballot_sync(full, has);
+    if (pend == 0u) return;
+    const uint32_t w = s / d.W, slot = i * E.wslots + (w - E.t_w0[i]);
+    const unsigned long long key = has ? window_key(v, t, s - w * d.W) : 0ull;
+    while (pend) {
+        const uint32_t lead = __ffs(pend) - 1;
+        const uint32_t sl = __shfl_sync(full, slot, lead);
+        const bool mine = has && slot == sl;
+        unsigned long long k = mine ? key : 0ull;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(full, k, off);
+            k = o > k ? o : k;
+        }
+        if (lane == lead) {
+            atomicMax(&E.s_key[sl], k);
+            E.s_pos[sl] = 1u;
+        }
+        pend &= ~__ballot_sync(full, mine);
+    }
+}
+
+// Each row's largest certain lower bound (mlb > 0 where pos) into its window
+// slot.  The warp's rows are consecutive, so for W >= 32 they meet at most two
+// windows: two warp reductions and at most two shared atomics.
+__device__ __forceinline__ void warp_window_mlb(const Epi& E, uint32_t W, uint32_t wslot, float mlb, bool pos)
+{
+    const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31;
+    const uint32_t pm = __ballot_sync(full, pos);
+    if (pm == 0u) return;
+    if (W < 32) {
+        if (pos) {
+            atomicMax(&E.s_mlb[wslot], __float_as_int(mlb));
+            E.s_pos[wslot] = 1u;
+        }
+        return;
+    }
+    const uint32_t lead = __ffs(pm) - 1;
+    const uint32_t wa = __shfl_sync(full, wslot, lead);
+    const bool in_a = pos && wslot == wa, in_b = pos && wslot != wa;
+    const int ma = __reduce_max_sync(full, in_a ? __float_as_int(mlb) : 0);
+    const int mb = __reduce_max_sync(full, in_b ? __float_as_int(mlb) : 0);
+    const uint32_t bm = __ballot_sync(full, in_b);
+    if (lane == lead) {
+        atomicMax(&E.s_mlb[wa], ma);
+        E.s_pos[wa] = 1u;
+    }
+    if (bm != 0u && lane == __ffs(bm) - 1) {
+        atomicMax(&E.s_mlb[wslot], mb);
+        E.s_pos[wslot] = 1u;
+    }
+}
+
 // Pass 1 of the epilogue over `ntiles` tiles (TMEM columns tbase + i * Np, this
-// thread's row): estimates stored; samples of uncertain sign (lazy) or that can
-// be positive (not lazy) queued; the window slots' largest lower bounds.
+// thread's row) for the template groups t0 = tfirst, tfirst + tstep, ... (4
+// templates each): estimates stored; samples of uncertain sign (lazy) or that
+// can be positive (not lazy) queued; each window slot's largest certain lower
+// bound.  The TMEM load of the next group is in flight while a group is
+// evaluated; it completes before any queueing call.
 __device__ __forceinline__ void epi_pass1(const TcParams& P, const Epi& E, uint32_t tbase, uint32_t ntiles,
-                                          uint32_t row, bool lazy)
+                                          uint32_t row, bool lazy, uint32_t tfirst, uint32_t tstep)
 {
     const Dims& d = P.d;
     for (uint32_t i = 0; i < ntiles; ++i) {
@@ -294,29 +345,55 @@ __device__ __forceinline__ void epi_pass1(const TcParams& P, const Epi& E, uint3
         const bool valid = row < E.t_rows[i];
         const bool live = valid && (uint64_t)s + d.W < d.N;
         const uint32_t wslot = valid ? i * E.wslots + (s / d.W - E.t_w0[i]) : 0u;
+        const float* bnd = E.bnd + i * d.M;
+        float mlb = 0.f;
+        bool pos = false;
+        uint32_t r[4];
+        if (tfirst < d.M) {
+            tmem_ld4_issue(tbase + i * P.Np + tfirst, r);
+            tmem_wait4(r);
+        }
 #pragma unroll 1
-        for (uint32_t t0 = 0; t0 < d.M; t0 += 4) {
-            float v[4];
-            tmem_ld4(tbase + i * P.Np + t0, v);
+        for (uint32_t t0 = tfirst; t0 < d.M; t0 += tstep) {
+            float est[4];
+            bool need[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) est[e] = __uint_as_float(r[e]);
+            const bool more = t0 + tstep < d.M;
+            if (more) tmem_ld4_issue(tbase + i * P.Np + t0 + tstep, r);
+            bool any = false;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const uint32_t t = t0 + e;
+                need[e] = false;
                 if (t >= d.M) break;   // the same for every lane
-                const float b = E.sbias[t];
-                const float est = v[e] + b;
-                const float bd = E.bnd[i * d.M + t];
-                const bool certain = lazy && live && est - bd > 0.f;
-                const bool need = live && !(est + bd <= 0.f) && !certain;
+                est[e] += E.sbias[t];
+                const float bd = bnd[t];
+                const bool certain = lazy && live && est[e] - bd > 0.f;
+                need[e] = live && !(est[e] + bd <= 0.f) && !certain;
                 if (certain) {
-                    atomicMax(&E.s_mlb[wslot], __float_as_int(est - bd));
-                    E.s_pos[wslot] = 1u;
+                    mlb = fmaxf(mlb, est[e] - bd);
+                    pos = true;
                 }
-                bool here = false;
-                const float out = enqueue(P, E, need, t, i, row, s, b, live ? est : 0.f, &here);
-                if (here && lazy) note_exact(d, E, out, t, i, s);
-                if (valid) P.L[(uint64_t)t * d.N + s] = out;
+                if (!live) est[e] = 0.f;
+                if (valid && !need[e]) P.L[(uint64_t)t * d.N + s] = est[e];
+                any |= need[e];
+            }
+            any = __any_sync(0xffffffffu, any);
+            if (more) tmem_wait4(r);
+            if (any) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const uint32_t t = t0 + e;
+                    if (t >= d.M) break;
+                    bool here = false;
+                    const float out = enqueue(P, E, need[e], t, i, row, s, E.sbias[t], est[e], &here);
+                    if (here && lazy) note_exact(d, E, out, t, i, s);
+                    if (need[e]) P.L[(uint64_t)t * d.N + s] = out;
+                }
             }
         }
+        if (lazy) warp_window_mlb(E, d.W, wslot, mlb, pos);
     }
 }
 
@@ -324,7 +401,7 @@ __device__ __forceinline__ void epi_pass1(const TcParams& P, const Epi& E, uint3
 // its largest lower bound) are queued; the other certainly positive samples keep
 // their estimate and flag their (window, template) row.
 __device__ __forceinline__ void epi_pass2(const TcParams& P, const Epi& E, uint32_t tbase, uint32_t ntiles,
-                                          uint32_t row)
+                                          uint32_t row, uint32_t tfirst, uint32_t tstep)
 {
     const Dims& d = P.d;
     for (uint32_t i = 0; i < ntiles; ++i) {
@@ -333,38 +410,61 @@ __device__ __forceinline__ void epi_pass2(const TcParams& P, const Epi& E, uint3
         const bool live = valid && (uint64_t)s + d.W < d.N;
         const uint32_t wslot = valid ? i * E.wslots + (s / d.W - E.t_w0[i]) : 0u;
         const float mlb = __int_as_float(E.s_mlb[wslot]);
+        const float* bnd = E.bnd + i * d.M;
+        uint8_t* inex = E.s_inex + (size_t)wslot * d.M;
+        uint32_t r[4];
+        if (tfirst < d.M) {
+            tmem_ld4_issue(tbase + i * P.Np + tfirst, r);
+            tmem_wait4(r);
+        }
 #pragma unroll 1
-        for (uint32_t t0 = 0; t0 < d.M; t0 += 4) {
-            float v[4];
-            tmem_ld4(tbase + i * P.Np + t0, v);
+        for (uint32_t t0 = tfirst; t0 < d.M; t0 += tstep) {
+            float est[4];
+            bool cont[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) est[e] = __uint_as_float(r[e]);
+            const bool more = t0 + tstep < d.M;
+            if (more) tmem_ld4_issue(tbase + i * P.Np + t0 + tstep, r);
+            bool any = false;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const uint32_t t = t0 + e;
+                cont[e] = false;
                 if (t >= d.M) break;
-                const float b = E.sbias[t];
-                const float est = v[e] + b;
-                const float bd = E.bnd[i * d.M + t];
-                const bool certain = live && est - bd > 0.f;
-                const bool contender = certain && est + bd >= mlb;
-                bool here = false;
-                const float out = enqueue(P, E, contender, t, i, row, s, b, est, &here);
-                if (here) {
-                    note_exact(d, E, out, t, i, s);
-                    P.L[(uint64_t)t * d.N + s] = out;
+                est[e] += E.sbias[t];
+                const float bd = bnd[t];
+                const bool certain = live && est[e] - bd > 0.f;
+                cont[e] = certain && est[e] + bd >= mlb;
+                if (certain && !cont[e]) inex[t] = 1;
+                any |= cont[e];
+            }
+            any = __any_sync(0xffffffffu, any);
+            if (more) tmem_wait4(r);
+            if (any) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const uint32_t t = t0 + e;
+                    if (t >= d.M) break;
+                    bool here = false;
+                    const float out = enqueue(P, E, cont[e], t, i, row, s, E.sbias[t], est[e], &here);
+                    if (here) {
+                        note_exact(d, E, out, t, i, s);
+                        P.L[(uint64_t)t * d.N + s] = out;
+                    }
                 }
-                if (certain && !contender) E.s_inex[wslot * d.M + t] = 1;
             }
         }
     }
 }
 
-// Exact recomputation of the queued runs, one warp per run (warps w0, w0 + ws,
-// ...): lanes 0..3 carry the run's four samples' sums, each adding its products
-// one at a time in the reference order (channel-major, taps ascending), over the
-// template's non-zero channels (an all-zero channel adds exact zeros); the
-// template row of the next such channel is loaded while the current one is
-// summed and staged in the warp's shared scratch (2 x 128 floats).  Vt: the
-// strips transposed to channel-major rows (channel c of tile i at (i Cp + c) R8).
+// Exact recomputation of the queued runs, one warp per entry (warps w0, w0 +
+// wstride, ...): lane k carries the sum of row 32 quarter + k, adding its
+// products one at a time in the reference order (channel-major, taps ascending)
+// over the template's non-zero channels (an all-zero channel adds exact zeros);
+// the template row of the next such channel is loaded while the current one is
+// summed and staged in the warp's shared scratch (2 x 128 floats).  Lanes whose
+// row is not in the entry's mask compute a value nobody reads.  Vt: the strips
+// transposed to channel-major rows (channel c of tile i at (i Cp + c) R8).
 __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, const float* Vt, uint32_t nq,
                                                uint32_t w0, uint32_t wstride, float* scratch, bool lazy)
 {
@@ -372,9 +472,9 @@ __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, 
     const uint32_t lane = threadIdx.x & 31, W = d.W, Wp = (W + 3) & ~3u, Cp = P.Cq * 4;
     float* tw = scratch;   // this warp's [2][128]
     for (uint32_t qi = w0; qi < nq; qi += wstride) {
-        const uint32_t e = E.fq[qi];
-        const uint32_t t = e >> 14, i = (e >> 11) & 7u, r0 = (e >> 4) & 127u, mask = e & 0xFu;
-        const uint32_t k = lane & 3u;   // lanes 4..31 repeat lanes 0..3 and are discarded
+        const unsigned long long e = E.fq[qi];
+        const uint32_t mask = (uint32_t)(e >> 32), lo = (uint32_t)e;
+        const uint32_t t = lo >> 5, i = (lo >> 2) & 7u, r = (lo & 3u) * 32u + lane;
         float acc = E.sbias[t];
         const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
         const float* tnr = P.tnorm + (uint64_t)t * d.C;
@@ -401,7 +501,7 @@ __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, 
                 }
             }
             const float* tr = tw + buf * 128u;
-            const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r0 + k;
+            const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r;
 #pragma unroll 4
             for (uint32_t j = 0; j < W; ++j) acc = __fadd_rn(acc, __fmul_rn(tr[j], vr[j]));
             if (cn < d.C) {
@@ -412,11 +512,10 @@ __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, 
             buf ^= 1u;
             c = cn;
         }
-        if (lane < 4 && ((mask >> lane) & 1u)) {
-            const uint32_t sk = E.t_s0[i] + r0 + lane;
-            P.L[(uint64_t)t * d.N + sk] = acc;
-            if (lazy) note_exact(d, E, acc, t, i, sk);
-        }
+        const bool mine = (mask >> lane) & 1u;
+        const uint32_t sk = E.t_s0[i] + r;
+        if (mine) P.L[(uint64_t)t * d.N + sk] = acc;
+        if (lazy) warp_note_exact(d, E, mine, acc, t, i, sk);
         __syncwarp();
     }
 }
@@ -475,8 +574,9 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
     float* snorm = reinterpret_cast<float*>(t_rows + P.ntiles);   // [ntiles][C]
     float* bnd = snorm + P.ntiles * d.C;                          // [ntiles][M]
     float* sbias = bnd + P.ntiles * d.M;                          // [M]
-    uint32_t* fq = reinterpret_cast<uint32_t*>(sbias + d.M);      // [kFixCap] runs: t | tile | row | mask
-    uint32_t* nfq = fq + kFixCap;
+    unsigned long long* fq = reinterpret_cast<unsigned long long*>(
+        (reinterpret_cast<uintptr_t>(sbias + d.M) + 7) & ~(uintptr_t)7);   // [kFixCap] queued runs
+    uint32_t* nfq = reinterpret_cast<uint32_t*>(fq + kFixCap);
     uint32_t* t_w0 = nfq + 1;                                      // [ntiles] first window of each tile
     int* s_mlb = reinterpret_cast<int*>(t_w0 + P.ntiles);          // [ntiles][wslots] max lower bound (float bits)
     uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_mlb + P.ntiles * P.wslots);   // [ntiles][wslots]
@@ -605,10 +705,10 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
             const uint32_t row = qd * 32 + lane;
             const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
             const uint32_t tbase = tmem + ((qd * 32) << 16);
-            epi_pass1(P, E, tbase, P.ntiles, row, P.lazy != 0);
+            epi_pass1(P, E, tbase, P.ntiles, row, P.lazy != 0, 0u, 4u);
             if (P.lazy) {
                 asm volatile("bar.sync 1, 128;" ::: "memory");
-                epi_pass2(P, E, tbase, P.ntiles, row);
+                epi_pass2(P, E, tbase, P.ntiles, row, 0u, 4u);
             }
         }
         tc_fence_before();
@@ -670,11 +770,14 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
 // Persistent tensor-core likelihood (the pursuit's passes, lazy exactness).
 //
 // One CTA per SM walks batches of B tiles.  The voltage strips and the TMEM
-// accumulators are double-buffered, so while the 4 epilogue warps finish batch
-// k (estimates, bounds, window maxima, exact recomputation of the queued runs
+// accumulators are double-buffered, so while the epilogue warps finish batch k
+// (estimates, bounds, window maxima, exact recomputation of the queued runs
 // from the strips, window keys), the bulk-copy warp and the MMA warp already run
 // batch k+1; and each pass of the template ring feeds B tiles (as many as one
-// TMEM buffer of 256 columns holds) instead of one CTA's two.
+// TMEM buffer of 256 columns holds) instead of one CTA's two.  NE warpgroups run
+// the epilogue: warpgroup g evaluates the template groups 4g, 4g + 4 NE, ... of
+// all 128 rows (each of its warps reads its TMEM lane quarter), so every SM
+// sub-partition has NE epilogue warps to interleave.
 //   barriers: a_full[s]   strips (and the batch's tile list) of buffer s loaded
 //             a_empty[s]  the epilogue is done with buffer s's strips
 //             acc_full[s] the MMAs of buffer s's batch completed (tcgen05.commit)
@@ -682,19 +785,26 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
 //             b_full/b_empty  the template ring, stage counter running across batches
 // The results are those of lik_tc_kernel in lazy mode.
 // ---------------------------------------------------------------------------
-// True on every epilogue thread (named barrier 1, 128 threads) iff p holds on
-// all of them: the epilogue's loop decisions stay uniform, so no thread leaves a
+template <uint32_t N>
+__device__ __forceinline__ void epi_sync()
+{
+    asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory");
+}
+
+// True on every epilogue thread (named barrier 1, N threads) iff p holds on all
+// of them: the epilogue's loop decisions stay uniform, so no thread leaves a
 // loop whose named barriers the others still wait at.
+template <uint32_t N>
 __device__ __forceinline__ bool epi_all(bool p)
 {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.and.pred q, 1, 128, p;\n\t"
+        "bar.red.and.pred q, 1, %2, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}"
         : "=r"(r)
-        : "r"((uint32_t)p)
+        : "r"((uint32_t)p), "n"(N)
         : "memory");
     return r != 0;
 }
@@ -704,8 +814,12 @@ struct PersistParams {
     uint32_t nbatches;
 };
 
-__global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistParams Q)
+constexpr uint32_t persist_threads(int ne) { return 64u + 128u * (uint32_t)ne; }
+
+template <int NE>
+__global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(PersistParams Q)
 {
+    constexpr uint32_t EPI = 128u * NE;   // epilogue threads
     extern __shared__ __align__(1024) unsigned char smem[];
     const TcParams& P = Q.P;
     const Dims& d = P.d;
@@ -725,21 +839,21 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
     uint64_t* drain = bars + 8;       // the MMA warp's last commit, on an error
     uint64_t* b_full = bars + 9;
     uint64_t* b_empty = b_full + P.stages;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(b_empty + P.stages);
+    unsigned long long* fq = reinterpret_cast<unsigned long long*>(b_empty + P.stages);   // [kFixCap] queued runs
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fq + kFixCap);
     uint32_t* err = tmem_slot + 1;
-    uint32_t* meta = err + 1;                                      // [2][3][B]: s0, rows, first window
+    uint32_t* nfq = err + 1;
+    uint32_t* meta = nfq + 1;                                      // [2][3][B]: s0, rows, first window
     float* snorm = reinterpret_cast<float*>(meta + 6 * B);         // [B][C]
     float* bnd = snorm + B * d.C;                                  // [B][M]
     float* sbias = bnd + B * d.M;                                  // [M]
-    uint32_t* fq = reinterpret_cast<uint32_t*>(sbias + d.M);       // [kFixCap]: t << 14 | tile << 11 | row << 4 | mask
-    uint32_t* nfq = fq + kFixCap;
-    int* s_mlb = reinterpret_cast<int*>(nfq + 1);                  // [B][wslots]
+    int* s_mlb = reinterpret_cast<int*>(sbias + d.M);              // [B][wslots]
     uint32_t* s_pos = reinterpret_cast<uint32_t*>(s_mlb + B * P.wslots);
     unsigned long long* s_key = reinterpret_cast<unsigned long long*>(
         (reinterpret_cast<uintptr_t>(s_pos + B * P.wslots) + 7) & ~(uintptr_t)7);
     uint8_t* s_inex = reinterpret_cast<uint8_t*>(s_key + B * P.wslots);   // [B][wslots][M]
     float* scratch = reinterpret_cast<float*>(
-        (reinterpret_cast<uintptr_t>(s_inex + B * P.wslots * d.M) + 15) & ~(uintptr_t)15);   // [4 warps][256]
+        (reinterpret_cast<uintptr_t>(s_inex + B * P.wslots * d.M) + 15) & ~(uintptr_t)15);   // [4 NE warps][256]
 
     const uint32_t ksteps = d.W * (P.Cq / 2);
     const uint32_t ngroups = (ksteps + P.group - 1) / P.group;
@@ -844,50 +958,56 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
             }
         }
     } else {
-        const uint32_t et = threadIdx.x - 64, ew = warp - 2;   // 128 epilogue threads, warps 0..3
-        const uint32_t qd = warp & 3, row = qd * 32 + lane;
+        const uint32_t et = threadIdx.x - 64, ew = warp - 2;   // epilogue threads and warps
+        const uint32_t qd = warp & 3, row = qd * 32 + lane, grp = ew >> 2;
         for (uint32_t batch = blockIdx.x, it = 0; batch < Q.nbatches; batch += gridDim.x, ++it) {
             const uint32_t s = it & 1, use = it >> 1;
-            if (!epi_all(*(volatile uint32_t*)err == 0)) break;
-            if (!epi_all(mbar_wait(&a_full[s], use & 1))) { if (et == 0) atomicOr(err, 4u); break; }
+            if (!epi_all<EPI>(*(volatile uint32_t*)err == 0)) break;
+            if (!epi_all<EPI>(mbar_wait(&a_full[s], use & 1))) { if (et == 0) atomicOr(err, 4u); break; }
             const uint32_t* t_s0 = meta + s * 3 * B;
             const uint32_t* t_rows = t_s0 + B;
             const uint32_t* t_w0 = t_rows + B;
             unsigned char* Ab = A + s * B * tile_bytes;
-            // per-batch scratch, norms of the strips and the bounds
+            // per-batch scratch, norms of the strips (4 threads per tile channel) and the bounds
             if (et == 0) *nfq = 0;
-            for (uint32_t e = et; e < B * P.wslots; e += 128) {
+            for (uint32_t e = et; e < B * P.wslots; e += EPI) {
                 s_mlb[e] = 0;
                 s_pos[e] = 0;
                 s_key[e] = 0ull;
             }
-            for (uint32_t e = et; e < B * P.wslots * d.M; e += 128) s_inex[e] = 0;
-            for (uint32_t e = et; e < B * d.C; e += 128) {
-                const uint32_t i = e / d.C, c = e % d.C;
-                const float* col = reinterpret_cast<const float*>(Ab + i * tile_bytes + (c / 4) * strip_bytes) + (c % 4);
-                const uint32_t nr = t_rows[i] ? t_rows[i] + d.W - 1 : 0;
+            for (uint32_t e = et; e < B * P.wslots * d.M; e += EPI) s_inex[e] = 0;
+            const uint32_t nsub = B * d.C * 4;
+            for (uint32_t e0 = 0; e0 < nsub; e0 += EPI) {
+                const uint32_t e = e0 + et;
                 float acc = 0.f;
-                for (uint32_t r = 0; r < nr; ++r) acc = fmaf(col[r * 4], col[r * 4], acc);
-                snorm[e] = sqrtf(acc) * 1.0001f;
+                if (e < nsub) {
+                    const uint32_t ic = e >> 2, k = e & 3u, i = ic / d.C, c = ic - i * d.C;
+                    const float* col = reinterpret_cast<const float*>(Ab + i * tile_bytes + (c / 4) * strip_bytes) + (c % 4);
+                    const uint32_t nr = t_rows[i] ? t_rows[i] + d.W - 1 : 0;
+                    for (uint32_t r = k; r < nr; r += 4) acc = fmaf(col[r * 4], col[r * 4], acc);
+                }
+                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                if (e < nsub && (e & 3u) == 0) snorm[e >> 2] = sqrtf(acc) * 1.0001f;
             }
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            for (uint32_t e = et; e < B * d.M; e += 128) {
+            epi_sync<EPI>();
+            for (uint32_t e = et; e < B * d.M; e += EPI) {
                 const uint32_t i = e / d.M, t = e % d.M;
                 float a = 0.f;
                 for (uint32_t c = 0; c < d.C; ++c) a = fmaf(P.tnorm[t * d.C + c], snorm[i * d.C + c], a);
                 bnd[e] = P.k_a * a * 1.0001f + P.k_b * fabsf(sbias[t]);
             }
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            if (!epi_all(mbar_wait(&acc_full[s], use & 1))) { if (et == 0) atomicOr(err, 8u); break; }
+            epi_sync<EPI>();
+            if (!epi_all<EPI>(mbar_wait(&acc_full[s], use & 1))) { if (et == 0) atomicOr(err, 8u); break; }
             tc_fence_after();
             const uint32_t tbase = tmem + ((qd * 32) << 16) + s * 256u;
             const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
-            epi_pass1(P, E, tbase, B, row, true);
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            epi_pass2(P, E, tbase, B, row);
+            epi_pass1(P, E, tbase, B, row, true, 4u * grp, 4u * NE);
+            epi_sync<EPI>();
+            epi_pass2(P, E, tbase, B, row, 4u * grp, 4u * NE);
             // TMEM buffer s read: the MMAs of batch it+2 may use it
             tc_fence_before();
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            epi_sync<EPI>();
             if (et == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[s])) : "memory");
             // exact recomputation of the queued runs from buffer s's strips, transposed in
             // place to channel-major rows (the MMAs of this batch are complete)
@@ -895,14 +1015,13 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
             if (et == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
             if (nq > 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                transpose_strips(Ab, B * P.Cq, P.R8, et, 128u, [] { asm volatile("bar.sync 1, 128;" ::: "memory"); });
-                const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
-                recompute_runs(P, E, reinterpret_cast<const float*>(Ab), nq, ew, 4u, scratch + ew * 256u, true);
+                transpose_strips(Ab, B * P.Cq, P.R8, et, EPI, [] { epi_sync<EPI>(); });
+                recompute_runs(P, E, reinterpret_cast<const float*>(Ab), nq, ew, 4u * NE, scratch + ew * 256u, true);
             }
             const uint32_t W = d.W;
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            epi_sync<EPI>();
             // publish the batch's window maxima, positive flags and estimate flags
-            for (uint32_t e = et; e < B * P.wslots; e += 128) {
+            for (uint32_t e = et; e < B * P.wslots; e += EPI) {
                 const uint32_t i = e / P.wslots, j = e - i * P.wslots;
                 if (t_rows[i] == 0 || j > (t_s0[i] + t_rows[i] - 1) / W - t_w0[i]) continue;
                 const uint32_t w = t_w0[i] + j;
@@ -914,7 +1033,7 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
                     if (s_pos[e]) P.wpos[w] = 1;
                 }
             }
-            for (uint32_t e = et; e < B * P.wslots * d.M; e += 128) {
+            for (uint32_t e = et; e < B * P.wslots * d.M; e += EPI) {
                 const uint32_t slot = e / d.M, t = e - slot * d.M;
                 const uint32_t i = slot / P.wslots, j = slot - i * P.wslots;
                 if (t_rows[i] == 0 || j > (t_s0[i] + t_rows[i] - 1) / W - t_w0[i]) continue;
@@ -924,7 +1043,7 @@ __global__ void __launch_bounds__(kThreads, 1) lik_tc_persist_kernel(PersistPara
             // strips of buffer s (written through the generic proxy by the transposition)
             // go back to the bulk copies
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            epi_sync<EPI>();
             if (et == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&a_empty[s])) : "memory");
         }
     }
@@ -1193,7 +1312,7 @@ bool tc_config(const Dims& d, TcConfig* c)
         // after the MMAs the ring is the exact recomputation's scratch: 6 warps x 1 KB
         while (c->stages * c->group * kstep < 6 * 1024 + 256) ++c->group;
         const size_t misc = 8 + c->ntiles * 8 + (size_t)c->ntiles * (d.C + d.M) * 4 + (size_t)d.M * 4 +
-                            (size_t)kFixCap * 4 + 4 + (size_t)c->ntiles * 4 + (size_t)c->ntiles * win_slots(d.W) * (16 + d.M) + 8 +
+                            (size_t)kFixCap * 8 + 8 + 4 + (size_t)c->ntiles * 4 + (size_t)c->ntiles * win_slots(d.W) * (16 + d.M) + 8 +
                             1024;
         auto total = [&](uint32_t stages) { return strips + stages * c->group * kstep + (2 + 2 * stages) * 8 + misc; };
         if (fit < 4 && !tu.lik_stages) {
@@ -1274,37 +1393,51 @@ int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const
     return FBP_OK;
 }
 
-// Persistent launch shape: tiles per batch (one TMEM buffer of 256 columns) and
-// the deepest template ring that fits the shared memory.  False when one buffer
-// holds fewer than two tiles or the caller asked for a tile count.
+// Persistent launch shape: tiles per batch (one TMEM buffer of 256 columns), the
+// deepest template ring that fits the shared memory, and the epilogue
+// warpgroups.  False when one buffer holds fewer than two tiles or the caller
+// asked for a tile count.
 struct PersistConfig {
-    uint32_t B, stages, group;
+    uint32_t B, stages, group, ne;
     size_t smem;
 };
 
 bool persist_config(const Dims& d, const TcConfig& c, PersistConfig* p)
 {
-    if (tuning().lik_tiles != 0) return false;
+    const fbp_tuning& tu = tuning();
+    if (tu.lik_tiles != 0) return false;
     uint32_t B = std::min<uint32_t>(8, 256 / c.Np);
     if (B < 2) return false;
+    const uint32_t ne = tu.lik_epi ? tu.lik_epi : 2;
     const size_t tile = (size_t)c.Cq * c.R8 * 16, kstep = (size_t)c.Np * 32;
     const uint32_t ws = win_slots(d.W);
     for (; B >= 2; --B) {
-        const size_t misc = (9 + 0) * 8 + 8 + 6 * B * 4 + (size_t)B * (d.C + d.M) * 4 + (size_t)d.M * 4 +
-                            (size_t)kFixCap * 4 + 4 + (size_t)B * ws * 8 + 8 + (size_t)B * ws * 8 +
-                            (size_t)B * ws * d.M + 16 + 4 * 256 * 4 + 1024;
+        const size_t misc = 9 * 8 + (size_t)kFixCap * 8 + 12 + 6 * B * 4 + (size_t)B * (d.C + d.M) * 4 +
+                            (size_t)d.M * 4 + (size_t)B * ws * 8 + 8 + (size_t)B * ws * 8 + (size_t)B * ws * d.M +
+                            16 + (size_t)4 * ne * 256 * 4 + 1024;
         const size_t budget = 220 * 1024;
-        uint32_t group = c.group, stages = tuning().lik_stages ? tuning().lik_stages : 8;
+        uint32_t group = c.group, stages = tu.lik_stages ? tu.lik_stages : 8;
         auto total = [&](uint32_t st, uint32_t g) { return 2 * B * tile + st * g * kstep + 2 * st * 8 + misc; };
         while (stages > 2 && total(stages, group) > budget) --stages;
         if (total(stages, group) > budget) continue;
         p->B = B;
         p->stages = stages;
         p->group = group;
+        p->ne = ne;
         p->smem = std::max<size_t>(total(stages, group), 116 * 1024);   // one CTA per SM (it takes all TMEM)
         return true;
     }
     return false;
+}
+
+template <int NE>
+static int launch_persist(const PersistParams& Q, uint32_t grid, size_t smem, cudaStream_t st)
+{
+    FBP_CUDA(allow_max_dyn_smem(lik_tc_persist_kernel<NE>));
+    KScope ks(&fbp_chunk_stats::ms_lik_tc, st);
+    lik_tc_persist_kernel<NE><<<grid, persist_threads(NE), smem, st>>>(Q);
+    FBP_CUDA(cudaGetLastError());
+    return FBP_OK;
 }
 
 int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T, const float* bias,
@@ -1371,10 +1504,13 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
         int dev = 0, sms = 148;
         FBP_CUDA(cudaGetDevice(&dev));
         FBP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        FBP_CUDA(allow_max_dyn_smem(lik_tc_persist_kernel));
         const uint32_t grid = std::min<uint32_t>(Q.nbatches, (uint32_t)sms);
-        KScope ks(&fbp_chunk_stats::ms_lik_tc, st);
-        lik_tc_persist_kernel<<<grid, kThreads, pc.smem, st>>>(Q);
+        switch (pc.ne) {
+            case 1: FBP_TRY(launch_persist<1>(Q, grid, pc.smem, st)); break;
+            case 3: FBP_TRY(launch_persist<3>(Q, grid, pc.smem, st)); break;
+            case 4: FBP_TRY(launch_persist<4>(Q, grid, pc.smem, st)); break;
+            default: FBP_TRY(launch_persist<2>(Q, grid, pc.smem, st)); break;
+        }
     } else {
         FBP_CUDA(allow_max_dyn_smem(lik_tc_kernel));
         const uint32_t grid = (uint32_t)((items + c.ntiles - 1) / c.ntiles);

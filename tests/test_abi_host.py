@@ -34,7 +34,7 @@ def test_header_declares_exports():
 def test_library_exports_every_declared_symbol(lib):
     for name in declared_functions():
         assert hasattr(lib, name), name
-    assert lib.fbp_abi_version() == _native.ABI_VERSION == 3
+    assert lib.fbp_abi_version() == _native.ABI_VERSION == 4
 
 
 def test_workspace_bytes(lib):
@@ -133,6 +133,8 @@ def test_tuning_validation(lib):
     assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
     t = _native.FbpTuning(0, 0, 0, 3)   # group size not a power of two
     assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
-    t = _native.FbpTuning(1, 2, 4, 4)
+    t = _native.FbpTuning(0, 0, 0, 0, 5)   # more than four epilogue warpgroups
+    assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_E_ARG
+    t = _native.FbpTuning(1, 2, 4, 4, 3)
     assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_OK
     assert lib.fbp_set_tuning(None) == _native.FBP_OK
