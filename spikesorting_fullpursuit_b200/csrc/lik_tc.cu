@@ -122,6 +122,30 @@ __device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint6
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
+// Issues the MMAs of k-steps [k0, k0 + nk) for `ntl` tiles.  k-step k is (tap
+// j, channel pair qp) = (k / nqp, k % nqp); A of tile i is its strip seen from
+// row j of channel block 2 qp, B the staged template k-step.  The descriptors
+// advance in their start-address field (16-byte units): shared addresses stay
+// below 256 KB, so the 14-bit field never carries into the next one.
+__device__ __forceinline__ void issue_ksteps(uint32_t d_tmem, uint32_t Np, uint32_t ntl, uint64_t adesc0,
+                                             uint32_t tile_units, uint32_t qp_units, uint64_t bdesc0,
+                                             uint32_t kstep_units, uint32_t k0, uint32_t nk, uint32_t nqp,
+                                             uint32_t idesc)
+{
+    uint32_t j = k0 / nqp, qp = k0 - j * nqp;
+    uint64_t bd = bdesc0;
+    for (uint32_t kq = 0; kq < nk; ++kq) {
+        const uint64_t ad = adesc0 + j + qp * qp_units;
+        const uint32_t acc = (k0 + kq) > 0 ? 1u : 0u;
+        for (uint32_t i = 0; i < ntl; ++i) umma_tf32(d_tmem + i * Np, ad + i * tile_units, bd, idesc, acc);
+        bd += kstep_units;
+        if (++qp == nqp) {
+            qp = 0;
+            ++j;
+        }
+    }
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -656,16 +680,9 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
                 if (!mbar_wait(&b_full[st], round & 1)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t k0 = g * P.group, nk = min(P.group, ksteps - k0);
-                for (uint32_t kq = 0; kq < nk; ++kq) {
-                    const uint32_t k = k0 + kq;
-                    const uint32_t j = k / (P.Cq / 2), qp = k % (P.Cq / 2);
-                    const uint64_t bdesc = umma_desc(b_base + st * stage_bytes + kq * kstep_bytes, P.Np * 16, 128);
-                    for (uint32_t i = 0; i < P.ntiles; ++i) {
-                        const uint32_t a_addr = a_base + i * tile_bytes + (2 * qp) * strip_bytes + j * 16;
-                        const uint64_t adesc = umma_desc(a_addr, strip_bytes, 128);
-                        umma_tf32(tmem + i * P.Np, adesc, bdesc, idesc, k > 0 ? 1u : 0u);
-                    }
-                }
+                issue_ksteps(tmem, P.Np, P.ntiles, umma_desc(a_base, strip_bytes, 128), tile_bytes >> 4,
+                             (2 * strip_bytes) >> 4, umma_desc(b_base + st * stage_bytes, P.Np * 16, 128),
+                             kstep_bytes >> 4, k0, nk, P.Cq / 2, idesc);
                 umma_commit(&b_empty[st]);
                 ++issued;
             }
@@ -942,15 +959,9 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
                     if (!mbar_wait(&b_full[st], round & 1)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t k0 = g * P.group, nk = min(P.group, ksteps - k0);
-                    for (uint32_t kq = 0; kq < nk; ++kq) {
-                        const uint32_t k = k0 + kq;
-                        const uint32_t j = k / (P.Cq / 2), qp = k % (P.Cq / 2);
-                        const uint64_t bdesc = umma_desc(r_base + st * stage_bytes + kq * kstep_bytes, P.Np * 16, 128);
-                        for (uint32_t i = 0; i < B; ++i) {
-                            const uint32_t a_addr = a_base + i * tile_bytes + (2 * qp) * strip_bytes + j * 16;
-                            umma_tf32(dcol + i * P.Np, umma_desc(a_addr, strip_bytes, 128), bdesc, idesc, k > 0 ? 1u : 0u);
-                        }
-                    }
+                    issue_ksteps(dcol, P.Np, B, umma_desc(a_base, strip_bytes, 128), tile_bytes >> 4,
+                                 (2 * strip_bytes) >> 4, umma_desc(r_base + st * stage_bytes, P.Np * 16, 128),
+                                 kstep_bytes >> 4, k0, nk, P.Cq / 2, idesc);
                     umma_commit(&b_empty[st]);
                 }
                 umma_commit(&acc_full[s]);   // completes once every MMA issued so far has
