@@ -117,6 +117,7 @@ bool make_layout(const fbp_dims* d, uint32_t flags, Layout* L)
         L->off_tt_hi = take(L->Mp * W * L->Cp * 4);    // templates as [W][Cp/8][2][Mp][4] fp32
         L->off_tpad = take(M * C * ((W + 3) / 4 * 4) * 4);   // templates as [M][C][W rounded up to 4]
         L->off_tnorm = take(M * C * 4);
+        L->off_tchm = take(M * 8);
         uint64_t cap = M * N / 4;
         if (cap > (32ull << 20)) cap = 32ull << 20;
         L->n_fix_cap = cap + 4096;

@@ -102,7 +102,7 @@ struct Layout {
     size_t off_has, off_newval, off_pidx, off_plab, off_pwin, off_pconf, off_keys;
     size_t off_blk, off_status;
     // tensor-core likelihood (mode 1)
-    size_t off_vt_hi, off_tt_hi, off_tpad, off_fix, off_tnorm;
+    size_t off_vt_hi, off_tt_hi, off_tpad, off_fix, off_tnorm, off_tchm;
     uint64_t Cp, Mp, n_fix_cap, vq_rows;
     // lazy exactness of the tensor-core likelihood: per-window maximum keys and
     // positive flags, and per (window, template) "row holds estimates" flags

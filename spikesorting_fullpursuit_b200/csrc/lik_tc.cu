@@ -164,6 +164,7 @@ struct TcParams {
     const float* Tq;      // [W][Cq/2][2][Np][4]
     const float* bias;    // [M]
     const float* tnorm;   // [M][C] channel norms of the templates
+    const unsigned long long* tchm;   // [M] channels c < 64 where template t is not all zero (C <= 64)
     const float* Tp;      // [M][C][Wp] templates, taps padded to a multiple of 4 (exact recomputation)
     const uint32_t* list; // listed windows (mode 1) or null (mode 0: contiguous tiles)
     uint32_t nitems;      // tiles (mode 0) or listed windows (mode 1)
@@ -502,8 +503,19 @@ __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, 
         float acc = E.sbias[t];
         const float* tb = P.Tp + (uint64_t)t * d.C * Wp;
         const float* tnr = P.tnorm + (uint64_t)t * d.C;
-        uint32_t c = 0;
-        while (c < d.C && tnr[c] == 0.f) ++c;
+        // the template's non-zero channels in order: from its mask (C <= 64), else by norms
+        const bool bym = d.C <= 64;
+        const unsigned long long chm = bym ? P.tchm[t] : 0ull;
+        auto next_chan = [&](uint32_t from) -> uint32_t {
+            if (bym) {
+                const unsigned long long rest = from < 64 ? chm & (~0ull << from) : 0ull;
+                return rest ? (uint32_t)(__ffsll((long long)rest) - 1) : d.C;
+            }
+            uint32_t c = from;
+            while (c < d.C && tnr[c] == 0.f) ++c;
+            return c;
+        };
+        uint32_t c = next_chan(0);
         float tn[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -515,8 +527,7 @@ __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, 
         for (int q = 0; q < 4; ++q) tw[lane + 32u * q] = tn[q];
         __syncwarp();
         while (c < d.C) {
-            uint32_t cn = c + 1;
-            while (cn < d.C && tnr[cn] == 0.f) ++cn;
+            const uint32_t cn = next_chan(c + 1);
             if (cn < d.C) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -526,7 +537,7 @@ __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, 
             }
             const float* tr = tw + buf * 128u;
             const float* vr = Vt + ((size_t)i * Cp + c) * P.R8 + r;
-#pragma unroll 4
+#pragma unroll 8
             for (uint32_t j = 0; j < W; ++j) acc = __fadd_rn(acc, __fmul_rn(tr[j], vr[j]));
             if (cn < d.C) {
 #pragma unroll
@@ -831,7 +842,7 @@ struct PersistParams {
     uint32_t nbatches;
 };
 
-constexpr uint32_t persist_threads(int ne) { return 64u + 128u * (uint32_t)ne; }
+constexpr uint32_t persist_threads(int ne) { return 96u + 128u * (uint32_t)ne; }
 
 template <int NE>
 __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(PersistParams Q)
@@ -853,8 +864,8 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
     uint64_t* a_empty = bars + 2;     // [2]
     uint64_t* acc_full = bars + 4;    // [2]
     uint64_t* acc_empty = bars + 6;   // [2]
-    uint64_t* drain = bars + 8;       // the MMA warp's last commit, on an error
-    uint64_t* b_full = bars + 9;
+    uint64_t* drain = bars + 8;       // [2] each MMA warp's last commit, on an error
+    uint64_t* b_full = bars + 10;
     uint64_t* b_empty = b_full + P.stages;
     unsigned long long* fq = reinterpret_cast<unsigned long long*>(b_empty + P.stages);   // [kFixCap] queued runs
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fq + kFixCap);
@@ -878,14 +889,14 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
         for (int s = 0; s < 2; ++s) {
             mbar_init(&a_full[s], 1);
             mbar_init(&a_empty[s], 1);
-            mbar_init(&acc_full[s], 1);
+            mbar_init(&acc_full[s], 2);   // one commit per MMA warp
             mbar_init(&acc_empty[s], 1);
+            mbar_init(&drain[s], 1);
         }
         for (uint32_t s = 0; s < P.stages; ++s) {
             mbar_init(&b_full[s], 1);
-            mbar_init(&b_empty[s], 1);
+            mbar_init(&b_empty[s], 2);    // one commit per MMA warp
         }
-        mbar_init(drain, 1);
         *err = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -940,36 +951,41 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
                 if (!ok) { atomicOr(err, 1u); break; }
             }
         }
-    } else if (warp == 1) {
+    } else if (warp == 1 || warp == 2) {
+        // two MMA warps: warp 1 the batch's first (B + 1) / 2 tiles, warp 2 the others
+        // (one issuing thread is limited to about one MMA per 60 cycles)
         if (lane == 0) {
             const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((P.Np >> 3) << 17) | ((kTile >> 4) << 24);
             const uint32_t r_base = smem_u32(R);
+            const uint32_t B1 = (B + 1) / 2, t0 = warp == 1 ? 0u : B1, ntl = warp == 1 ? B1 : B - B1;
+            const uint32_t ebit = warp == 1 ? 2u : 16u;
             uint32_t gtot = 0;
             for (uint32_t batch = blockIdx.x, it = 0; batch < Q.nbatches; batch += gridDim.x, ++it) {
                 const uint32_t s = it & 1, use = it >> 1;
                 if (*(volatile uint32_t*)err) break;
-                if (!mbar_wait(&a_full[s], use & 1)) { atomicOr(err, 2u); break; }
-                if (use > 0 && !mbar_wait(&acc_empty[s], (use - 1) & 1)) { atomicOr(err, 2u); break; }
+                if (!mbar_wait(&a_full[s], use & 1)) { atomicOr(err, ebit); break; }
+                if (use > 0 && !mbar_wait(&acc_empty[s], (use - 1) & 1)) { atomicOr(err, ebit); break; }
                 tc_fence_after();
-                const uint32_t a_base = smem_u32(A + s * B * tile_bytes);
-                const uint32_t dcol = tmem + s * 256u;
+                const uint32_t a_base = smem_u32(A + s * B * tile_bytes) + t0 * tile_bytes;
+                const uint32_t dcol = tmem + s * 256u + t0 * P.Np;
                 bool ok = true;
                 for (uint32_t g = 0; g < ngroups; ++g, ++gtot) {
                     const uint32_t st = gtot % P.stages, round = gtot / P.stages;
                     if (!mbar_wait(&b_full[st], round & 1)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t k0 = g * P.group, nk = min(P.group, ksteps - k0);
-                    issue_ksteps(dcol, P.Np, B, umma_desc(a_base, strip_bytes, 128), tile_bytes >> 4,
-                                 (2 * strip_bytes) >> 4, umma_desc(r_base + st * stage_bytes, P.Np * 16, 128),
-                                 kstep_bytes >> 4, k0, nk, P.Cq / 2, idesc);
+                    if (ntl > 0)
+                        issue_ksteps(dcol, P.Np, ntl, umma_desc(a_base, strip_bytes, 128), tile_bytes >> 4,
+                                     (2 * strip_bytes) >> 4, umma_desc(r_base + st * stage_bytes, P.Np * 16, 128),
+                                     kstep_bytes >> 4, k0, nk, P.Cq / 2, idesc);
                     umma_commit(&b_empty[st]);
                 }
-                umma_commit(&acc_full[s]);   // completes once every MMA issued so far has
-                if (!ok) { atomicOr(err, 2u); break; }
+                umma_commit(&acc_full[s]);   // completes once every MMA this thread issued has
+                if (!ok) { atomicOr(err, ebit); break; }
             }
         }
     } else {
-        const uint32_t et = threadIdx.x - 64, ew = warp - 2;   // epilogue threads and warps
+        const uint32_t et = threadIdx.x - 96, ew = warp - 3;   // epilogue threads and warps
         const uint32_t qd = warp & 3, row = qd * 32 + lane, grp = ew >> 2;
         for (uint32_t batch = blockIdx.x, it = 0; batch < Q.nbatches; batch += gridDim.x, ++it) {
             const uint32_t s = it & 1, use = it >> 1;
@@ -1009,7 +1025,8 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
                 bnd[e] = P.k_a * a * 1.0001f + P.k_b * fabsf(sbias[t]);
             }
             epi_sync<EPI>();
-            if (!epi_all<EPI>(mbar_wait(&acc_full[s], use & 1))) { if (et == 0) atomicOr(err, 8u); break; }
+            // one poller per warp; the barrier and the fence below order the TMEM reads after it
+            if (!epi_all<EPI>(lane != 0 || mbar_wait(&acc_full[s], use & 1))) { if (et == 0) atomicOr(err, 8u); break; }
             tc_fence_after();
             const uint32_t tbase = tmem + ((qd * 32) << 16) + s * 256u;
             const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
@@ -1060,13 +1077,13 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
     }
     __syncthreads();
     if (threadIdx.x == 0 && *err) atomicOr(&P.status->error, 0x200u | *err);
+    if ((warp == 1 || warp == 2) && lane == 0 && *err) {
+        // this thread's MMAs may still be in flight: a last commit arrives once all are done
+        umma_commit(&drain[warp - 1]);
+        mbar_wait(&drain[warp - 1], 0);
+    }
+    __syncthreads();
     if (warp == 1) {
-        if (lane == 0 && *err) {
-            // MMAs may still be in flight: a last commit arrives once all are done
-            umma_commit(drain);
-            mbar_wait(drain, 0);
-        }
-        __syncwarp();
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
     }
@@ -1260,8 +1277,18 @@ __global__ void voltage_repack_kernel(Dims d, const float* __restrict__ V, uint3
 // Tq[j][qp][h][n][e] = T[n][(2qp+h)*4+e][j]; Tp[t][c][j] = T[t][c][j] (zero for
 // j >= W); tnorm[t][c] = |T[t][c][:]|.
 __global__ void template_pack_kernel(Dims d, const float* __restrict__ T, uint32_t Cq, uint32_t Np, float* Tq,
-                                     float* Tp, float* tnorm)
+                                     float* Tp, float* tnorm, unsigned long long* tchm)
 {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < d.M; t += gridDim.x * blockDim.x) {
+        unsigned long long m = 0ull;
+        for (uint32_t c = 0; c < d.C && c < 64; ++c) {
+            const float* r = T + ((uint64_t)t * d.C + c) * d.W;
+            bool nz = false;
+            for (uint32_t j = 0; j < d.W && !nz; ++j) nz = r[j] != 0.f;
+            if (nz) m |= 1ull << c;
+        }
+        tchm[t] = m;
+    }
     const uint32_t Wp = (d.W + 3) & ~3u;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (uint64_t)d.M * d.C * Wp;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -1381,7 +1408,7 @@ int launch_tc_prepare_templates(const Dims& d, const Work& w, const float* T, cu
     const Layout& L = *w.lay;
     count_launch();
     template_pack_kernel<<<256, 256, 0, st>>>(d, T, c.Cq, c.Np, w.at<float>(L.off_tt_hi), w.at<float>(L.off_tpad),
-                                              w.at<float>(L.off_tnorm));
+                                              w.at<float>(L.off_tnorm), w.at<unsigned long long>(L.off_tchm));
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }
@@ -1417,13 +1444,14 @@ bool persist_config(const Dims& d, const TcConfig& c, PersistConfig* p)
 {
     const fbp_tuning& tu = tuning();
     if (tu.lik_tiles != 0) return false;
-    uint32_t B = std::min<uint32_t>(8, 256 / c.Np);
+    // an even tile count: the two MMA warps take half each
+    uint32_t B = std::min<uint32_t>(8, 256 / c.Np) & ~1u;
     if (B < 2) return false;
     const uint32_t ne = tu.lik_epi ? tu.lik_epi : 2;
     const size_t tile = (size_t)c.Cq * c.R8 * 16, kstep = (size_t)c.Np * 32;
     const uint32_t ws = win_slots(d.W);
-    for (; B >= 2; --B) {
-        const size_t misc = 9 * 8 + (size_t)kFixCap * 8 + 12 + 6 * B * 4 + (size_t)B * (d.C + d.M) * 4 +
+    for (; B >= 2; B -= 2) {
+        const size_t misc = 10 * 8 + (size_t)kFixCap * 8 + 12 + 6 * B * 4 + (size_t)B * (d.C + d.M) * 4 +
                             (size_t)d.M * 4 + (size_t)B * ws * 8 + 8 + (size_t)B * ws * 8 + (size_t)B * ws * d.M +
                             16 + (size_t)4 * ne * 256 * 4 + 1024;
         const size_t budget = 220 * 1024;
@@ -1468,6 +1496,7 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     P.Tq = w.at<float>(L.off_tt_hi);
     P.bias = bias;
     P.tnorm = w.at<float>(L.off_tnorm);
+    P.tchm = w.at<unsigned long long>(L.off_tchm);
     P.Tp = w.at<float>(L.off_tpad);
     const bool all = nlist == d.nw;
     P.list = all ? nullptr : list;
