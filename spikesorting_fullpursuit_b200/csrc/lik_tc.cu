@@ -122,27 +122,50 @@ __device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint6
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-// Issues the MMAs of k-steps [k0, k0 + nk) for `ntl` tiles.  k-step k is (tap
-// j, channel pair qp) = (k / nqp, k % nqp); A of tile i is its strip seen from
-// row j of channel block 2 qp, B the staged template k-step.  The descriptors
-// advance in their start-address field (16-byte units): shared addresses stay
-// below 256 KB, so the 14-bit field never carries into the next one.
-__device__ __forceinline__ void issue_ksteps(uint32_t d_tmem, uint32_t Np, uint32_t ntl, uint64_t adesc0,
-                                             uint32_t tile_units, uint32_t qp_units, uint64_t bdesc0,
-                                             uint32_t kstep_units, uint32_t k0, uint32_t nk, uint32_t nqp,
-                                             uint32_t idesc)
+// Issues the MMAs of k-steps [k0, k0 + nk) for NT tiles.  k-step k is (tap j,
+// channel pair qp) = (k / nqp, k % nqp); A of tile i is its strip seen from row j
+// of channel block 2 qp, B the staged template k-step.  The descriptors advance
+// in their start-address field (16-byte units): shared addresses stay below
+// 256 KB, so the 14-bit field never carries into the next one.  The tile loop is
+// unrolled: one issuing thread's dependent address arithmetic, not the tensor
+// core, otherwise sets the MMA rate at these sizes.
+template <int NT>
+__device__ __forceinline__ void issue_ksteps_n(uint32_t d_tmem, uint32_t Np, uint64_t adesc0, uint32_t tile_units,
+                                               uint32_t qp_units, uint64_t bdesc0, uint32_t kstep_units, uint32_t k0,
+                                               uint32_t nk, uint32_t nqp, uint32_t idesc)
 {
     uint32_t j = k0 / nqp, qp = k0 - j * nqp;
     uint64_t bd = bdesc0;
+    uint32_t dd[NT];
+    uint64_t ao[NT];
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+        dd[i] = d_tmem + i * Np;
+        ao[i] = (uint64_t)i * tile_units;
+    }
     for (uint32_t kq = 0; kq < nk; ++kq) {
         const uint64_t ad = adesc0 + j + qp * qp_units;
         const uint32_t acc = (k0 + kq) > 0 ? 1u : 0u;
-        for (uint32_t i = 0; i < ntl; ++i) umma_tf32(d_tmem + i * Np, ad + i * tile_units, bd, idesc, acc);
+#pragma unroll
+        for (int i = 0; i < NT; ++i) umma_tf32(dd[i], ad + ao[i], bd, idesc, acc);
         bd += kstep_units;
         if (++qp == nqp) {
             qp = 0;
             ++j;
         }
+    }
+}
+
+__device__ __forceinline__ void issue_ksteps(uint32_t d_tmem, uint32_t Np, uint32_t ntl, uint64_t adesc0,
+                                             uint32_t tile_units, uint32_t qp_units, uint64_t bdesc0,
+                                             uint32_t kstep_units, uint32_t k0, uint32_t nk, uint32_t nqp,
+                                             uint32_t idesc)
+{
+    switch (ntl) {
+        case 1: issue_ksteps_n<1>(d_tmem, Np, adesc0, tile_units, qp_units, bdesc0, kstep_units, k0, nk, nqp, idesc); break;
+        case 2: issue_ksteps_n<2>(d_tmem, Np, adesc0, tile_units, qp_units, bdesc0, kstep_units, k0, nk, nqp, idesc); break;
+        case 3: issue_ksteps_n<3>(d_tmem, Np, adesc0, tile_units, qp_units, bdesc0, kstep_units, k0, nk, nqp, idesc); break;
+        default: issue_ksteps_n<4>(d_tmem, Np, adesc0, tile_units, qp_units, bdesc0, kstep_units, k0, nk, nqp, idesc); break;
     }
 }
 
@@ -1455,8 +1478,12 @@ bool persist_config(const Dims& d, const TcConfig& c, PersistConfig* p)
                             (size_t)d.M * 4 + (size_t)B * ws * 8 + 8 + (size_t)B * ws * 8 + (size_t)B * ws * d.M +
                             16 + (size_t)4 * ne * 256 * 4 + 1024;
         const size_t budget = 220 * 1024;
-        uint32_t group = c.group, stages = tu.lik_stages ? tu.lik_stages : 8;
         auto total = [&](uint32_t st, uint32_t g) { return 2 * B * tile + st * g * kstep + 2 * st * 8 + misc; };
+        // template stages of up to 16 k-steps (fewer, longer MMA runs per stage), at least
+        // three in flight; then as many stages as fit
+        uint32_t group = tu.lik_group ? tu.lik_group : 16;
+        while (group > 1 && total(3, group) > budget) group >>= 1;
+        uint32_t stages = tu.lik_stages ? tu.lik_stages : 8;
         while (stages > 2 && total(stages, group) > budget) --stages;
         if (total(stages, group) > budget) continue;
         p->B = B;
