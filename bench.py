@@ -365,8 +365,9 @@ def main():
             kernels[name] = {"ms": ms, "bound": "fp32-simt", "achieved": ach, "peak": fma_peak,
                              "unit": "TFLOP/s", "frac": ach / fma_peak, "work": what,
                              "peak_kind": "nominal FP32 FMA issue rate at the sampled clock"}
-    # the roofline line reports the dominant kernel among those with a throughput bound
-    dom = max((k for k in kernels if kernels[k]["bound"] != "latency"), key=lambda k: kernels[k]["ms"])
+    # the roofline line reports the dominant kernel among those bound by the tensor pipe
+    # or by HBM; the FP32-pipe and latency-bound kernels are in `kernels`
+    dom = max((k for k in kernels if kernels[k]["bound"] in ("tensor", "hbm")), key=lambda k: kernels[k]["ms"])
     roof = dict(kernels[dom])
     # DRAM bytes (read + write) per launch: ncu's per-unit figure from the captures in
     # profiles/ (60 s slice of this workload) times the units of an average launch here
@@ -377,8 +378,11 @@ def main():
         traffic = per_unit[0] * units / max(1, st_stage["passes"])   # bytes per launch
         traffic_detail = {"bytes_per_unit": per_unit[0], "unit": per_unit[1] + " window",
                           "launches_per_step": st_stage["passes"], "source": per_unit[2]}
+    slowest = max(kernels, key=lambda k: kernels[k]["ms"])
     roof.update({"kernel": dom, "traffic": traffic, "traffic_detail": traffic_detail, "peak_kind": peak_kind,
-                 "note": "peak = measured dense bf16 (TF32 nominal is half of it); hbm = measured copy"})
+                 "note": ("peak = measured dense bf16 burst (the kernel computes in TF32, whose nominal rate is half)"
+                          if roof["bound"] == "tensor" else "peak = measured HBM copy bandwidth"),
+                 "slowest_kernel": slowest})
     launches = int(st_fast["launches"]) * args.steps
 
     cpu = None

@@ -579,25 +579,26 @@ __device__ __forceinline__ void recompute_runs(const TcParams& P, const Epi& E, 
 }
 
 // In-place transposition of `ntq` 4-channel blocks of R8 16-byte rows into
-// channel-major rows of R8 floats, by `nthr` threads (thread index `tid`) that
-// synchronise with `sync()` between reading a block and writing it.
-template <class Sync>
-__device__ __forceinline__ void transpose_strips(unsigned char* A, uint32_t ntq, uint32_t R8, uint32_t tid,
-                                                 uint32_t nthr, Sync sync)
+// channel-major rows of R8 floats.  A block's rows stay within its own bytes, so
+// one warp transposes a whole block (warps w0, w0 + nwarps, ...) with warp
+// synchronisation only; the caller synchronises the threads afterwards.
+__device__ __forceinline__ void transpose_strips(unsigned char* A, uint32_t ntq, uint32_t R8, uint32_t w0,
+                                                 uint32_t nwarps)
 {
+    const uint32_t lane = threadIdx.x & 31;
     const float4* src = reinterpret_cast<const float4*>(A);
     float* dst = reinterpret_cast<float*>(A);
-    for (uint32_t tq = 0; tq < ntq; ++tq) {
-        float4 vv[2];   // R8 <= 256 rows <= 2 * nthr (nthr >= 128)
+    for (uint32_t tq = w0; tq < ntq; tq += nwarps) {
+        float4 vv[8];   // R8 <= 256 rows
 #pragma unroll
-        for (uint32_t k = 0; k < 2; ++k) {
-            const uint32_t r = k * nthr + tid;
+        for (uint32_t k = 0; k < 8; ++k) {
+            const uint32_t r = k * 32 + lane;
             vv[k] = r < R8 ? src[(size_t)tq * R8 + r] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        sync();
+        __syncwarp();
 #pragma unroll
-        for (uint32_t k = 0; k < 2; ++k) {
-            const uint32_t r = k * nthr + tid;
+        for (uint32_t k = 0; k < 8; ++k) {
+            const uint32_t r = k * 32 + lane;
             if (r >= R8) continue;
             float* o = dst + (size_t)4 * tq * R8 + r;
             o[0] = vv[k].x;
@@ -605,7 +606,7 @@ __device__ __forceinline__ void transpose_strips(unsigned char* A, uint32_t ntq,
             o[2 * R8] = vv[k].z;
             o[3 * R8] = vv[k].w;
         }
-        sync();
+        __syncwarp();
     }
 }
 
@@ -783,7 +784,8 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
     if (nq > 0) {
         // the strips were written by bulk copies and read by the MMAs (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        transpose_strips(A, P.ntiles * P.Cq, P.R8, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+        transpose_strips(A, P.ntiles * P.Cq, P.R8, warp, blockDim.x >> 5);
+        __syncthreads();
         const Epi E{t_s0, t_rows, t_w0, sbias, bnd, s_mlb, s_pos, s_key, s_inex, fq, nfq, P.wslots};
         recompute_runs(P, E, reinterpret_cast<const float*>(A), nq, warp, blockDim.x >> 5,
                        reinterpret_cast<float*>(B) + warp * 256u, P.lazy != 0);
@@ -1066,7 +1068,8 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
             if (et == 0 && nq) atomicAdd(&P.status->n_fix_local, nq);
             if (nq > 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                transpose_strips(Ab, B * P.Cq, P.R8, et, EPI, [] { epi_sync<EPI>(); });
+                transpose_strips(Ab, B * P.Cq, P.R8, ew, 4u * NE);
+                epi_sync<EPI>();
                 recompute_runs(P, E, reinterpret_cast<const float*>(Ab), nq, ew, 4u * NE, scratch + ew * 256u, true);
             }
             const uint32_t W = d.W;
@@ -1470,7 +1473,7 @@ bool persist_config(const Dims& d, const TcConfig& c, PersistConfig* p)
     // an even tile count: the two MMA warps take half each
     uint32_t B = std::min<uint32_t>(8, 256 / c.Np) & ~1u;
     if (B < 2) return false;
-    const uint32_t ne = tu.lik_epi ? tu.lik_epi : 2;
+    const uint32_t ne = tu.lik_epi ? tu.lik_epi : 4;
     const size_t tile = (size_t)c.Cq * c.R8 * 16, kstep = (size_t)c.Np * 32;
     const uint32_t ws = win_slots(d.W);
     for (; B >= 2; B -= 2) {
@@ -1575,8 +1578,8 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
         switch (pc.ne) {
             case 1: FBP_TRY(launch_persist<1>(Q, grid, pc.smem, st)); break;
             case 3: FBP_TRY(launch_persist<3>(Q, grid, pc.smem, st)); break;
-            case 4: FBP_TRY(launch_persist<4>(Q, grid, pc.smem, st)); break;
-            default: FBP_TRY(launch_persist<2>(Q, grid, pc.smem, st)); break;
+            case 2: FBP_TRY(launch_persist<2>(Q, grid, pc.smem, st)); break;
+            default: FBP_TRY(launch_persist<4>(Q, grid, pc.smem, st)); break;
         }
     } else {
         FBP_CUDA(allow_max_dyn_smem(lik_tc_kernel));
