@@ -145,6 +145,24 @@ int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* voltage,
                      uint32_t* n_spikes, fbp_chunk_stats* stats, int32_t max_passes,
                      void* stream);
 
+/* fbp_pursue_chunk for a voltage that is still arriving on the device: the
+ * first pass's packing and likelihood run range by range behind the upload.
+ * ready_events[k] (a cudaEvent_t) completes once samples [0, ready_upto[k]) of
+ * every channel are in `voltage`; ready_flags[k] turns non-zero (written by the
+ * uploading host thread, read here with acquire ordering) once that event has
+ * been recorded, and this call waits on the host for it (at most 120 s, then
+ * FBP_E_ARG) before making `stream` wait for the event.  ready_upto strictly
+ * increasing, the last equal to n_samples.  Results are those of
+ * fbp_pursue_chunk.  No counterpart in the reference, whose host code uploads
+ * the whole chunk before its first kernel (binary_pursuit_parallel.py:611-616). */
+int fbp_pursue_chunk_staged(const fbp_dims* dims, uint32_t flags, float* voltage,
+                            const float* templates, const float* bias, const float* theta,
+                            void* workspace, size_t workspace_bytes,
+                            uint32_t* spike_idx, uint32_t* spike_lab, uint32_t capacity,
+                            uint32_t* n_spikes, fbp_chunk_stats* stats, int32_t max_passes,
+                            void* const* ready_events, const uint32_t* ready_upto,
+                            const uint32_t* ready_flags, uint32_t n_ready, void* stream);
+
 /* Adjusted clips: clips[k][c][j] = residual[c][idx_k + j] + templates[lab_k][c][j]
  * for idx_k + j < N, else left untouched (get_adjusted_clips,
  * binary_pursuit.cl:1088-1130).  clips is float32 [n][C*W]. */

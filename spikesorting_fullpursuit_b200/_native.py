@@ -24,7 +24,7 @@ FBP_PLAIN_FP32 = 0x2
 FBP_TIMING = 0x4
 
 # every function include/fbp.h declares
-EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_pursue_chunk",
+EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_pursue_chunk", "fbp_pursue_chunk_staged",
            "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc",
            "fbp_adjoint_loss", "fbp_adjoint_grad", "fbp_mean_clip", "fbp_bp_duplicates_workspace",
            "fbp_bp_duplicates", "fbp_separability", "fbp_gather_clips", "fbp_robust_template",
@@ -97,6 +97,9 @@ def lib():
     L.fbp_pursue_chunk.argtypes = [P(FbpDims), u32, vp, vp, vp, vp, vp, sz, vp, vp, u32,
                                    P(u32), P(FbpChunkStats), ctypes.c_int32, vp]
     L.fbp_pursue_chunk.restype = ctypes.c_int
+    L.fbp_pursue_chunk_staged.argtypes = [P(FbpDims), u32, vp, vp, vp, vp, vp, sz, vp, vp, u32,
+                                          P(u32), P(FbpChunkStats), ctypes.c_int32, vp, vp, vp, u32, vp]
+    L.fbp_pursue_chunk_staged.restype = ctypes.c_int
     L.fbp_adjusted_clips.argtypes = [P(FbpDims), vp, vp, vp, vp, u32, vp, vp]
     L.fbp_adjusted_clips.restype = ctypes.c_int
     L.fbp_likelihood.argtypes = [P(FbpDims), ctypes.c_int, vp, vp, vp, vp, u32, vp, vp, sz, vp]

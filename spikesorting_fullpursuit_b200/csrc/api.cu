@@ -6,9 +6,11 @@
 // and back every pass and compacts window lists with np.nonzero
 // (binary_pursuit_parallel.py:966-979, 1210-1251); here the lists are compacted
 // on the device and the host reads one 48-byte status word per pass.
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <utility>
 
 #include "fbp_internal.cuh"
@@ -215,15 +217,48 @@ extern "C" size_t fbp_workspace_bytes(const fbp_dims* dims, uint32_t flags)
     return L.bytes;
 }
 
-extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* voltage,
-                                const float* templates, const float* bias, const float* theta,
-                                void* workspace, size_t workspace_bytes, uint32_t* spike_idx,
-                                uint32_t* spike_lab, uint32_t capacity, uint32_t* n_spikes,
-                                fbp_chunk_stats* stats, int32_t max_passes, void* stream)
+namespace {
+
+// Voltage ranges arriving on the device (fbp_pursue_chunk_staged); n == 0: all present.
+struct Ready {
+    void* const* events = nullptr;
+    const uint32_t* upto = nullptr;
+    const uint32_t* flags = nullptr;
+    uint32_t n = 0;
+};
+
+// Host wait until the uploader has recorded event k, then the stream waits for it.
+int wait_ready(const Ready& R, uint32_t k, cudaStream_t st)
+{
+    if (R.flags) {
+        const auto t0 = std::chrono::steady_clock::now();
+        while (__atomic_load_n(&R.flags[k], __ATOMIC_ACQUIRE) == 0u) {
+            if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(120))
+                return fail(FBP_E_ARG, "voltage range " + std::to_string(k) + " was never marked ready");
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    }
+    FBP_CUDA(cudaStreamWaitEvent(st, static_cast<cudaEvent_t>(R.events[k]), 0));
+    return FBP_OK;
+}
+
+int pursue_chunk(const fbp_dims* dims, uint32_t flags, float* voltage, const float* templates, const float* bias,
+                 const float* theta, void* workspace, size_t workspace_bytes, uint32_t* spike_idx,
+                 uint32_t* spike_lab, uint32_t capacity, uint32_t* n_spikes, fbp_chunk_stats* stats,
+                 int32_t max_passes, const Ready& ready, void* stream)
 {
     g_err.clear();
     Layout lay;
     if (!make_layout(dims, flags, &lay)) return fail(FBP_E_ARG, "invalid dims");
+    if (ready.n > 0) {
+        if (!ready.events || !ready.upto) return fail(FBP_E_ARG, "null ready-range argument");
+        for (uint32_t k = 0; k < ready.n; ++k) {
+            if (!ready.events[k]) return fail(FBP_E_ARG, "null ready event");
+            if ((k > 0 && ready.upto[k] <= ready.upto[k - 1]) || ready.upto[k] > lay.N)
+                return fail(FBP_E_ARG, "ready ranges must increase up to n_samples");
+        }
+        if (ready.upto[ready.n - 1] != lay.N) return fail(FBP_E_ARG, "the last ready range must end at n_samples");
+    }
     if (!voltage || !templates || !bias || !theta || !workspace || !n_spikes)
         return fail(FBP_E_ARG, "null pointer argument");
     if (capacity > 0 && (!spike_idx || !spike_lab)) return fail(FBP_E_ARG, "null spike output");
@@ -259,7 +294,7 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     FBP_TRY(launch_iota(w.list(), d.nw, st));
     if (use_tc) {
         FBP_TRY(launch_tc_prepare_templates(d, w, templates, st));
-        FBP_TRY(launch_tc_update_voltage(d, w, voltage, nullptr, nullptr, 0, true, st));
+        if (ready.n == 0) FBP_TRY(launch_tc_update_voltage(d, w, voltage, nullptr, nullptr, 0, true, st));
     }
     if (lazy) FBP_CUDA(cudaMemsetAsync(w.base + lay.off_wflag, 0, lay.nw * lay.M, st));
     if (!plain && overlap) FBP_TRY(launch_overlap_tables(d, w, templates, st));
@@ -277,7 +312,28 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
         S.listed += nlist;
         FBP_CUDA(cudaMemsetAsync(&w.status()->chain_overflow, 0, 8, st));
         tm.start(timing, st, &S.ms_likelihood);
-        if (use_tc) {
+        if (pass == 1 && ready.n > 0) {
+            // first pass behind the upload: each arrived range is packed and the
+            // tiles whose strips it completes are pursued
+            const uint64_t R8 = use_tc ? tc_tile_rows(d) : 0, ntile = (lay.N + 127) / 128;
+            uint64_t packed = 0, tdone = 0;
+            for (uint32_t k = 0; k < ready.n; ++k) {
+                FBP_TRY(wait_ready(ready, k, st));
+                if (!use_tc) continue;
+                const bool last = k + 1 == ready.n;
+                const uint64_t r1 = last ? lay.vq_rows : ready.upto[k];
+                FBP_TRY(launch_tc_pack_range(d, w, voltage, packed, r1, st));
+                packed = r1;
+                const uint64_t tready = last ? ntile : (r1 >= R8 ? (r1 - R8) / 128 + 1 : 0);
+                if (tready > tdone) {
+                    uint64_t nfix = 0;
+                    FBP_TRY(launch_likelihood_tc(d, w, voltage, templates, bias, w.list(), nlist, w.L(), lazy, st,
+                                                 &nfix, tdone, tready - tdone));
+                    tdone = tready;
+                }
+            }
+            if (!use_tc) FBP_TRY(launch_likelihood_exact(d, voltage, templates, bias, w.list(), nlist, w.L(), st));
+        } else if (use_tc) {
             uint64_t nfix = 0;
             FBP_TRY(launch_likelihood_tc(d, w, voltage, templates, bias, w.list(), nlist, w.L(), lazy, st, &nfix));
         } else {
@@ -348,6 +404,39 @@ extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* vol
     S.launches = kclock().launches;
     *n_spikes = total;
     return FBP_OK;
+}
+
+}  // namespace
+
+extern "C" int fbp_pursue_chunk(const fbp_dims* dims, uint32_t flags, float* voltage,
+                                const float* templates, const float* bias, const float* theta,
+                                void* workspace, size_t workspace_bytes, uint32_t* spike_idx,
+                                uint32_t* spike_lab, uint32_t capacity, uint32_t* n_spikes,
+                                fbp_chunk_stats* stats, int32_t max_passes, void* stream)
+{
+    return pursue_chunk(dims, flags, voltage, templates, bias, theta, workspace, workspace_bytes, spike_idx,
+                        spike_lab, capacity, n_spikes, stats, max_passes, Ready{}, stream);
+}
+
+extern "C" int fbp_pursue_chunk_staged(const fbp_dims* dims, uint32_t flags, float* voltage,
+                                       const float* templates, const float* bias, const float* theta,
+                                       void* workspace, size_t workspace_bytes, uint32_t* spike_idx,
+                                       uint32_t* spike_lab, uint32_t capacity, uint32_t* n_spikes,
+                                       fbp_chunk_stats* stats, int32_t max_passes, void* const* ready_events,
+                                       const uint32_t* ready_upto, const uint32_t* ready_flags, uint32_t n_ready,
+                                       void* stream)
+{
+    if (n_ready == 0) {
+        g_err.clear();
+        return fail(FBP_E_ARG, "no ready ranges");
+    }
+    Ready r;
+    r.events = ready_events;
+    r.upto = ready_upto;
+    r.flags = ready_flags;
+    r.n = n_ready;
+    return pursue_chunk(dims, flags, voltage, templates, bias, theta, workspace, workspace_bytes, spike_idx,
+                        spike_lab, capacity, n_spikes, stats, max_passes, r, stream);
 }
 
 extern "C" int fbp_adjusted_clips(const fbp_dims* dims, const float* residual, const float* templates,

@@ -193,9 +193,14 @@ int launch_adjusted_clips(const Dims& d, const float* V, const float* T, const u
 
 // Tensor-core likelihood (lik_tc.cu)
 bool tc_supported(const Dims& d);
+// nlist == d.nw: the whole chunk, tiles [tile0, tile0 + tile_count) of 128 samples
 int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T,
                          const float* bias, const uint32_t* list, uint32_t nlist, float* L,
-                         bool lazy, cudaStream_t st, uint64_t* n_fix_out);
+                         bool lazy, cudaStream_t st, uint64_t* n_fix_out, uint64_t tile0 = 0,
+                         uint64_t tile_count = ~0ull);
+// Vq rows [r0, r1) from the voltage; the voltage rows a whole-chunk tile's strip reads
+int launch_tc_pack_range(const Dims& d, const Work& w, const float* V, uint64_t r0, uint64_t r1, cudaStream_t st);
+uint64_t tc_tile_rows(const Dims& d);
 // Lazy exactness: per-window argmax from the window keys, and the exact
 // recomputation of estimates whose voltage the coming residual changes in
 // windows the next pass does not relist.

@@ -191,6 +191,7 @@ struct TcParams {
     const float* Tp;      // [M][C][Wp] templates, taps padded to a multiple of 4 (exact recomputation)
     const uint32_t* list; // listed windows (mode 1) or null (mode 0: contiguous tiles)
     uint32_t nitems;      // tiles (mode 0) or listed windows (mode 1)
+    uint32_t tile0;       // mode 0: first tile of the range (tile k covers samples [128 (tile0 + k), +128))
     uint32_t rows;        // rows of each Vq channel block
     uint32_t Cq, Np, ntiles, R8, stages, ncols, group;   // group: k-steps per template stage
     float* L;
@@ -661,8 +662,8 @@ __global__ void __launch_bounds__(kThreads, 4) lik_tc_kernel(TcParams P)
         const uint64_t item = (uint64_t)blockIdx.x * P.ntiles + i;
         uint32_t s0 = 0, rows = 0;
         if (P.list == nullptr) {
-            const uint64_t st = item * kTile;
-            if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)kTile ? d.N - st : (uint64_t)kTile); }
+            const uint64_t st = ((uint64_t)P.tile0 + item) * kTile;
+            if (item < P.nitems && st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)kTile ? d.N - st : (uint64_t)kTile); }
         } else if (item < P.nitems) {
             const uint64_t st = (uint64_t)P.list[item] * d.W;
             if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)d.W ? d.N - st : (uint64_t)d.W); }
@@ -949,8 +950,8 @@ __global__ void __launch_bounds__(persist_threads(NE), 1) lik_tc_persist_kernel(
                     const uint64_t item = (uint64_t)batch * B + i;
                     uint32_t s0 = 0, rows = 0;
                     if (P.list == nullptr) {
-                        const uint64_t st = item * kTile;
-                        if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)kTile ? d.N - st : (uint64_t)kTile); }
+                        const uint64_t st = ((uint64_t)P.tile0 + item) * kTile;
+                        if (item < P.nitems && st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)kTile ? d.N - st : (uint64_t)kTile); }
                     } else if (item < P.nitems) {
                         const uint64_t st = (uint64_t)P.list[item] * d.W;
                         if (st < d.N) { s0 = (uint32_t)st; rows = (uint32_t)(d.N - st < (uint64_t)d.W ? d.N - st : (uint64_t)d.W); }
@@ -1265,18 +1266,21 @@ __global__ void lazy_fix_kernel(Dims d, const float* __restrict__ V, const float
 }
 
 // Vq[q][r][e] = V[4q+e][r] for r < N (zero elsewhere and for padding channels).
-__global__ void voltage_pack_kernel(Dims d, const float* __restrict__ V, uint32_t Cq, uint32_t rows, float4* Vq)
+// Vq rows [r0, r1) of every 4-channel block (rows past N are zeros).
+__global__ void voltage_pack_kernel(Dims d, const float* __restrict__ V, uint32_t Cq, uint32_t rows, uint32_t r0,
+                                    uint32_t r1, float4* Vq)
 {
-    const uint64_t total = (uint64_t)Cq * rows;
+    const uint32_t span = r1 - r0;
+    const uint64_t total = (uint64_t)Cq * span;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t q = (uint32_t)(i / rows), r = (uint32_t)(i % rows);
+        const uint32_t q = (uint32_t)(i / span), r = r0 + (uint32_t)(i % span);
         float x[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const uint32_t c = 4 * q + e;
             x[e] = (r < d.N && c < d.C) ? V[(uint64_t)c * d.N + r] : 0.f;
         }
-        Vq[i] = make_float4(x[0], x[1], x[2], x[3]);
+        Vq[(uint64_t)q * rows + r] = make_float4(x[0], x[1], x[2], x[3]);
     }
 }
 
@@ -1449,12 +1453,32 @@ int launch_tc_update_voltage(const Dims& d, const Work& w, const float* V, const
     float4* Vq = w.at<float4>(L.off_vt_hi);
     count_launch();
     if (all) {
-        voltage_pack_kernel<<<148 * 16, 256, 0, st>>>(d, V, c.Cq, (uint32_t)L.vq_rows, Vq);
+        voltage_pack_kernel<<<148 * 16, 256, 0, st>>>(d, V, c.Cq, (uint32_t)L.vq_rows, 0u, (uint32_t)L.vq_rows, Vq);
     } else if (n > 0) {
         voltage_repack_kernel<<<n < 65535u ? n : 65535u, 128, 0, st>>>(d, V, c.Cq, (uint32_t)L.vq_rows, idx, n, Vq);
     }
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
+}
+
+int launch_tc_pack_range(const Dims& d, const Work& w, const float* V, uint64_t r0, uint64_t r1, cudaStream_t st)
+{
+    TcConfig c;
+    if (!tc_config(d, &c) || r1 <= r0) return FBP_OK;
+    const Layout& L = *w.lay;
+    count_launch();
+    voltage_pack_kernel<<<148 * 16, 256, 0, st>>>(d, V, c.Cq, (uint32_t)L.vq_rows, (uint32_t)r0, (uint32_t)r1,
+                                                  w.at<float4>(L.off_vt_hi));
+    FBP_CUDA(cudaGetLastError());
+    return FBP_OK;
+}
+
+// Rows of the voltage a whole-chunk likelihood tile reads: tile k needs samples up to
+// 128 k + 128 + W - 1 (its strip, rounded up to 8 rows).
+uint64_t tc_tile_rows(const Dims& d)
+{
+    TcConfig c;
+    return tc_config(d, &c) ? c.R8 : 0;
 }
 
 // Persistent launch shape: tiles per batch (one TMEM buffer of 256 columns), the
@@ -1511,7 +1535,7 @@ static int launch_persist(const PersistParams& Q, uint32_t grid, size_t smem, cu
 
 int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const float* T, const float* bias,
                          const uint32_t* list, uint32_t nlist, float* Lk, bool lazy, cudaStream_t st,
-                         uint64_t* n_fix_out)
+                         uint64_t* n_fix_out, uint64_t tile0, uint64_t tile_count)
 {
     (void)n_fix_out;
     if (nlist == 0) return FBP_OK;
@@ -1530,8 +1554,11 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     P.Tp = w.at<float>(L.off_tpad);
     const bool all = nlist == d.nw;
     P.list = all ? nullptr : list;
-    const uint64_t items = all ? ((uint64_t)d.N + kTile - 1) / kTile : nlist;
+    const uint64_t tiles = ((uint64_t)d.N + kTile - 1) / kTile;
+    if (all && tile0 >= tiles) return FBP_OK;
+    const uint64_t items = all ? std::min<uint64_t>(tile_count, tiles - tile0) : nlist;
     P.nitems = (uint32_t)items;
+    P.tile0 = all ? (uint32_t)tile0 : 0u;
     P.rows = (uint32_t)L.vq_rows;
     P.Cq = c.Cq;
     P.Np = c.Np;
@@ -1555,7 +1582,7 @@ int launch_likelihood_tc(const Dims& d, const Work& w, const float* V, const flo
     P.wpos = lazy ? w.at<uint8_t>(L.off_wpos) : nullptr;
     P.wflag = lazy ? w.at<uint8_t>(L.off_wflag) : nullptr;
     P.wslots = win_slots(d.W);
-    if (lazy && all) {
+    if (lazy && all && tile0 == 0) {
         FBP_CUDA(cudaMemsetAsync(P.wkey, 0, (size_t)d.nw * 8, st));
         FBP_CUDA(cudaMemsetAsync(P.wpos, 0, (size_t)d.nw, st));
         FBP_CUDA(cudaMemsetAsync(P.wflag, 0, (size_t)d.nw * d.M, st));

@@ -41,6 +41,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import threading
 from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
@@ -128,7 +129,8 @@ class _Uploader:
 
     SLAB_FLOATS = 4 << 20    # 16 MB per slab
     N_SLABS = 16
-    N_THREADS = max(1, min(8, (os.cpu_count() or 2) // 2))
+    N_THREADS = max(1, min(16, os.cpu_count() or 2))
+    RANGE_SAMPLES = 1 << 20  # staged upload: samples of every channel per ready range
 
     def __init__(self, torch, dev):
         self.torch = torch
@@ -140,9 +142,7 @@ class _Uploader:
 
     def upload(self, host, dst):
         torch = self.torch
-        if self.slabs is None:
-            self.slabs = [torch.empty(self.SLAB_FLOATS, dtype=torch.float32, pin_memory=True)
-                          for _ in range(self.N_SLABS)]
+        self._ensure_slabs()
         C, N = host.shape
         step = self.SLAB_FLOATS
         pieces = [(c, a, min(N, a + step)) for c in range(C) for a in range(0, N, step)]
@@ -168,6 +168,78 @@ class _Uploader:
                     ev.record(self.stream)
                     self.events[k] = ev
         caller.wait_stream(self.stream)
+
+    def _ensure_slabs(self):
+        if self.slabs is None:
+            self.slabs = [self.torch.empty(self.SLAB_FLOATS, dtype=self.torch.float32, pin_memory=True)
+                          for _ in range(self.N_SLABS)]
+
+    def start_staged(self, host, dst):
+        """Upload ``host`` on a host thread, time range by time range.
+
+        Returns (events, upto, flags, finish): events[k] completes once samples
+        [0, upto[k]) of every channel are in ``dst``; flags[k] turns 1 once events[k]
+        is recorded (the library waits for it before waiting on the event);
+        ``finish()`` joins the thread and re-raises its error, if any."""
+        torch = self.torch
+        self._ensure_slabs()
+        C, N = host.shape
+        span = min(self.RANGE_SAMPLES, self.SLAB_FLOATS)
+        ranges = [(a, min(N, a + span)) for a in range(0, N, span)]
+        events = [torch.cuda.Event() for _ in ranges]
+        flags = np.zeros(len(ranges), dtype=np.uint32)
+        upto = np.array([b for _, b in ranges], dtype=np.uint32)
+        self.stream.wait_stream(torch.cuda.current_stream(self.dev))   # dst may still be read by earlier work
+        for ev in events:   # creates the CUDA events (torch makes them at the first record)
+            ev.record(self.stream)
+        half = self.N_SLABS // 2
+        failure = []
+
+        def run():
+            try:
+                with torch.cuda.device(self.dev):
+                    wave_no = 0
+                    for k, (a, b) in enumerate(ranges):
+                        pieces = [(c, a, b) for c in range(C)]
+                        for w0 in range(0, len(pieces), half):
+                            wave = pieces[w0:w0 + half]
+                            slots = [(wave_no % 2) * half + j for j in range(len(wave))]
+                            wave_no += 1
+                            for j in slots:
+                                if self.events[j] is not None:
+                                    self.events[j].synchronize()
+
+                            def fill(job):
+                                (c, x0, x1), j = job
+                                np.copyto(self.slabs[j].numpy()[:x1 - x0], host[c, x0:x1], casting="unsafe")
+
+                            list(self.pool.map(fill, zip(wave, slots)))
+                            with torch.cuda.stream(self.stream):
+                                for (c, x0, x1), j in zip(wave, slots):
+                                    dst[c, x0:x1].copy_(self.slabs[j][:x1 - x0], non_blocking=True)
+                                    ev = torch.cuda.Event()
+                                    ev.record(self.stream)
+                                    self.events[j] = ev
+                        events[k].record(self.stream)
+                        flags[k] = 1
+            except BaseException as e:   # the library must not wait for ranges that never come
+                failure.append(e)
+                with torch.cuda.device(self.dev):
+                    for k in range(len(ranges)):
+                        if not flags[k]:
+                            events[k].record(self.stream)
+                            flags[k] = 1
+
+        th = threading.Thread(target=run, daemon=True)
+        th.start()
+
+        def finish():
+            th.join()
+            torch.cuda.current_stream(self.dev).wait_stream(self.stream)
+            if failure:
+                raise failure[0]
+
+        return events, upto, flags, finish
 
     def close(self):
         self.pool.shutdown(wait=True)
@@ -204,7 +276,12 @@ class _Pursuer:
         C, N = host_chunk.shape
         d = _native.dims(C, N, self.M, self.W, self.S, self.wg)
         V = self.V[:, :N] if N == self.V.shape[1] else self.V.view(-1)[:C * N].view(C, N)
-        self.up.upload(host_chunk, V)
+        # the first pass runs behind the upload unless the autotuner must see the voltage first
+        ready = None
+        if self.tuning == "auto":
+            self.up.upload(host_chunk, V)
+        else:
+            ready = self.up.start_staged(host_chunk, V)
         nw = (N + self.W - 1) // self.W
         # every pass adds at most one spike per window
         most = nw * self.max_passes if self.max_passes > 0 else 0xFFFFFFFF
@@ -217,11 +294,11 @@ class _Pursuer:
                                         device=self.dev)
         autotune.apply(self.tuning)
         try:
-            return self._pursue(host_chunk, clips, V, d, N, nw, most, cap, stream, L)
+            return self._pursue(host_chunk, clips, V, d, N, nw, most, cap, stream, L, ready)
         finally:
             autotune.apply(None)
 
-    def _pursue(self, host_chunk, clips, V, d, N, nw, most, cap, stream, L):
+    def _pursue(self, host_chunk, clips, V, d, N, nw, most, cap, stream, L, ready=None):
         torch = self.torch
         C = V.shape[0]
         for attempt in range(MAX_CAPACITY_RETRIES + 1):
@@ -229,10 +306,24 @@ class _Pursuer:
             lab = torch.empty(cap, dtype=torch.int32, device=self.dev)
             n = ctypes.c_uint32(0)
             st = _native.FbpChunkStats()
-            rc = L.fbp_pursue_chunk(ctypes.byref(d), self.flags, _ptr(V), _ptr(self.T),
-                                    _ptr(self.bias), _ptr(self.theta), _ptr(self.ws),
-                                    self.ws.numel(), _ptr(idx), _ptr(lab), cap, ctypes.byref(n),
-                                    ctypes.byref(st), self.max_passes, stream)
+            if ready is not None:
+                events, upto, flags, finish = ready
+                ready = None
+                evp = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
+                try:
+                    rc = L.fbp_pursue_chunk_staged(ctypes.byref(d), self.flags, _ptr(V), _ptr(self.T),
+                                                   _ptr(self.bias), _ptr(self.theta), _ptr(self.ws),
+                                                   self.ws.numel(), _ptr(idx), _ptr(lab), cap, ctypes.byref(n),
+                                                   ctypes.byref(st), self.max_passes, evp,
+                                                   upto.ctypes.data_as(ctypes.c_void_p),
+                                                   flags.ctypes.data_as(ctypes.c_void_p), len(events), stream)
+                finally:
+                    finish()
+            else:
+                rc = L.fbp_pursue_chunk(ctypes.byref(d), self.flags, _ptr(V), _ptr(self.T),
+                                        _ptr(self.bias), _ptr(self.theta), _ptr(self.ws),
+                                        self.ws.numel(), _ptr(idx), _ptr(lab), cap, ctypes.byref(n),
+                                        ctypes.byref(st), self.max_passes, stream)
             if rc != _native.FBP_E_CAPACITY:
                 break
             if cap >= min(most, 0xFFFFFFFF) or attempt == MAX_CAPACITY_RETRIES:

@@ -66,6 +66,25 @@ def test_invalid_arguments_fail_before_any_device_call(lib):
     assert rc == _native.FBP_E_WORKSPACE
 
 
+def test_staged_pursuit_validates_ready_ranges_before_any_device_call(lib):
+    d = _native.dims(4, 5000, 4, 101, 100)
+    n = ctypes.c_uint32(0)
+    buf = ctypes.c_void_p(1 << 40)
+
+    def call(events, upto, k):
+        ev = (ctypes.c_void_p * max(1, len(events)))(*events)
+        up = np.array(upto or [0], dtype=np.uint32)
+        fl = np.ones(max(1, len(upto)), dtype=np.uint32)
+        return lib.fbp_pursue_chunk_staged(ctypes.byref(d), 0, buf, buf, buf, buf, buf, 1 << 40, buf, buf, 10,
+                                           ctypes.byref(n), None, 0, ev, up.ctypes.data_as(ctypes.c_void_p),
+                                           fl.ctypes.data_as(ctypes.c_void_p), k, None)
+
+    assert call([], [], 0) == _native.FBP_E_ARG                       # no ranges
+    assert call([None], [5000], 1) == _native.FBP_E_ARG               # null event
+    assert call([1, 1], [3000, 2000], 2) == _native.FBP_E_ARG         # not increasing
+    assert call([1, 1], [2000, 4000], 2) == _native.FBP_E_ARG         # does not reach n_samples
+    assert b"n_samples" in lib.fbp_last_error()
+
 @pytest.mark.parametrize("seed", range(40))
 def test_chunk_planner_matches_oracle(seed):
     rng = np.random.default_rng(seed)
