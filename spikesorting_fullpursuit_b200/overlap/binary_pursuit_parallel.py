@@ -127,10 +127,10 @@ class _Uploader:
     stream wait for the last piece.  The source may be any real dtype and any
     row-strided view: the float32 conversion happens in the slab copy."""
 
-    SLAB_FLOATS = 4 << 20    # 16 MB per slab
-    N_SLABS = 16
+    SLAB_FLOATS = 2 << 20    # 8 MB per slab
+    N_SLABS = 32
     N_THREADS = max(1, min(16, os.cpu_count() or 2))
-    RANGE_SAMPLES = 1 << 20  # staged upload: samples of every channel per ready range
+    RANGE_SAMPLES = 2 << 20  # staged upload: samples of every channel per ready range
 
     def __init__(self, torch, dev):
         self.torch = torch
