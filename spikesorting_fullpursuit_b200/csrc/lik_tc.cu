@@ -75,21 +75,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// As mbar_try_wait, letting the thread sleep until the phase completes or about
-// `ns` nanoseconds pass, so waiting warps leave their issue slots to the others.
-__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
-        : "memory");
-    return ok != 0;
-}
-
 __device__ __forceinline__ uint64_t global_ns()
 {
     uint64_t t;
@@ -98,15 +83,14 @@ __device__ __forceinline__ uint64_t global_ns()
 }
 
 // Bounded wait: false once the phase has not completed within kWaitNs of
-// device time (the global nanosecond timer), checked every 16 polls of at most
-// about 20 us of sleep each.
+// device time (the global nanosecond timer), checked every 64 polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (;;) {
-        for (int i = 0; i < 16; ++i)
-            if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try_wait(bar, parity)) return true;
         if (global_ns() - t0 > kWaitNs) return false;
     }
 }

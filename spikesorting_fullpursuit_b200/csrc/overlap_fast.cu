@@ -213,8 +213,7 @@ __global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
 {
     extern __shared__ __align__(16) float sm[];
     __shared__ uint32_t chans[256];
-    __shared__ uint8_t qmask[256];   // per staged channel: the group's templates that are not zero on it
-    __shared__ uint32_t s_nch, s_nqc;
+    __shared__ uint32_t s_nch;
     __shared__ uint32_t s_p[kPcWin];
     __shared__ int s_ok[kPcWin];
     const uint32_t S2 = 2 * d.S + 1, W = d.W, M = d.M;
@@ -223,18 +222,10 @@ __global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
         unsigned long long m = 0ull;
         for (uint32_t q = 0; q < Q; ++q)
             if (g0 + q < M) m |= chmask[perm[g0 + q]];
-        uint32_t n = 0, nqc = 0;
-        for (uint32_t c = 0; c < d.C; ++c) {
-            if (!(c >= 64 || ((m >> c) & 1ull))) continue;
-            uint32_t qm = 0;
-            for (uint32_t q = 0; q < Q; ++q)
-                if (g0 + q < M && (c >= 64 || ((chmask[perm[g0 + q]] >> c) & 1ull))) qm |= 1u << q;
-            chans[n] = c;
-            qmask[n++] = (uint8_t)qm;
-            nqc += __popc(qm);
-        }
+        uint32_t n = 0;
+        for (uint32_t c = 0; c < d.C; ++c)
+            if (c >= 64 || ((m >> c) & 1ull)) chans[n++] = c;
         s_nch = n;
-        s_nqc = nqc;
     }
     __syncthreads();
     const uint32_t Cu = s_nch;
@@ -291,18 +282,16 @@ __global__ void __launch_bounds__(kPcMaxWarps * 32, 2) partial_corr_kernel(
 #pragma unroll
                 for (int r = 0; r < kPcR; ++r) acc[q][r] = 0.f;
             const int vb = (int)b0 - gm.o;
-            if (jhi > jlo) macs += (unsigned long long)kPcR * (uint32_t)(jhi - jlo) * s_nqc;
+            if (jhi > jlo) macs += (unsigned long long)Q * kPcR * (uint32_t)(jhi - jlo) * Cu;
             for (uint32_t ci = 0; ci < Cu; ++ci) {
                 const float* vr = vw + (size_t)ci * gm.SLc;
                 const float* tr = Ts + (size_t)ci * Wp;
-                const uint32_t qm = qmask[ci];   // a template's all-zero channel adds nothing
                 for (int j0 = jlo; j0 < jhi; j0 += 4) {
                     const float4 va = *reinterpret_cast<const float4*>(vr + vb + j0);
                     const float4 vc = *reinterpret_cast<const float4*>(vr + vb + j0 + 4);
                     const float v[8] = {va.x, va.y, va.z, va.w, vc.x, vc.y, vc.z, vc.w};
 #pragma unroll
                     for (int q = 0; q < Q; ++q) {
-                        if (!((qm >> q) & 1u)) continue;
                         const float4 t4 = *reinterpret_cast<const float4*>(tr + (size_t)q * Cu * Wp + j0);
 #pragma unroll
                         for (int r = 0; r < kPcR; ++r) {
