@@ -69,6 +69,8 @@ def parse():
                    help="batched: launch shapes measured per segment shape (spikesorting_fullpursuit_b200.autotune)")
     p.add_argument("--duration", type=float, default=None, help="seconds of recording (default: config's)")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--gpu-synth", action="store_true",
+                   help="generate the recording's noise on the GPU (for the full-length dense 64-channel recording)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-s", type=float, default=1.0)
     p.add_argument("--adjoint", action="store_true",
@@ -216,7 +218,14 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=dev)
     assert args.warmup >= 3, "at least 3 warm-up steps"
-    V, si, sm, truth = synth.config_recording(args.config, seed=1 + rank, duration_s=args.duration)
+    if args.gpu_synth:
+        # recordings too long to band-pass on the host: noise drawn and filtered on the device
+        Vg, si, sm = synth.config_recording_gpu(args.config, seed=1 + rank, device=dev, duration_s=args.duration)
+        V = Vg.cpu().numpy()
+        del Vg
+        torch.cuda.empty_cache()
+    else:
+        V, si, sm, _ = synth.config_recording(args.config, seed=1 + rank, duration_s=args.duration)
     C, N = V.shape
     W = si["n_samples_per_chan"]
     S = W - 1
