@@ -106,11 +106,20 @@ def spike_trains(rng, n_units, duration_s, fs, rates, refractory_ms=1.5, overlap
     if overlap_frac > 0 and t_all.size > 1 and n_units > 1:
         n_move = int(round(overlap_frac * t_all.size))
         movers = rng.choice(t_all.size, size=n_move, replace=False)
+        # each unit's spikes are one contiguous block [lo, hi) of the concatenation, so
+        # the r-th spike of another unit is r below the block and r + (hi - lo) above it
+        counts = np.array([t.size for t in times], dtype=np.int64)
+        ends = np.cumsum(counts)
+        starts = ends - counts
+        n_all = t_all.size
         for i in movers:
-            others = np.flatnonzero(l_all != l_all[i])
-            if others.size == 0:
+            m = l_all[i]
+            lo, hi = int(starts[m]), int(ends[m])
+            n_other = n_all - (hi - lo)
+            if n_other == 0:
                 continue
-            j = others[rng.integers(0, others.size)]
+            r = int(rng.integers(0, n_other))
+            j = r if r < lo else r + (hi - lo)
             t_all[i] = t_all[j] + rng.uniform(-overlap_ms, overlap_ms) * 1e-3
         # restore each unit's refractory period after the moves
         keep = np.ones(t_all.size, dtype=bool)
