@@ -52,6 +52,8 @@ from ..processing.conversions import time_window_to_samples
 WORK_GROUP_SIZE = 256
 MAX_PASSES = 2048          # default pass limit of one chunk
 MAX_CAPACITY_RETRIES = 4   # re-runs of a chunk whose spikes outgrew the output buffers
+CAPACITY_PER_WINDOW = 16   # spike slots of a chunk's first attempt, per window ...
+CAPACITY_EXTRA = 1024      # ... plus these
 
 
 def plan_chunks(n_samples, n_chans, n_templates, template_samples_per_chan, sampling_rate,
@@ -283,9 +285,12 @@ class _Pursuer:
         else:
             ready = self.up.start_staged(host_chunk, V)
         nw = (N + self.W - 1) // self.W
-        # every pass adds at most one spike per window
+        # every pass adds at most one spike per window; dense probes end with about five
+        # spikes per window, so the first attempt holds 16 (8 B each, far below the
+        # likelihood's 4*M*W bytes per window) and a capacity retry, which pursues the
+        # chunk again, stays rare
         most = nw * self.max_passes if self.max_passes > 0 else 0xFFFFFFFF
-        cap = min(4 * nw + 1024, most, 0xFFFFFFFF)
+        cap = min(CAPACITY_PER_WINDOW * nw + CAPACITY_EXTRA, most, 0xFFFFFFFF)
         stream = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
         L = _native.lib()
         if self.tuning == "auto":

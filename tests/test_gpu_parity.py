@@ -167,6 +167,23 @@ def test_random_recordings_match_oracle(case, mode):
         assert np.array_equal(np.asarray(g), np.asarray(w)), case
 
 
+@pytest.mark.parametrize("mode", MODES)
+def test_capacity_retry_gives_the_same_result(mode, monkeypatch):
+    """A chunk whose spikes outgrow the first attempt's output buffers is
+    pursued again with a larger capacity; the result must not change."""
+    from spikesorting_fullpursuit_b200.overlap import binary_pursuit_parallel as bpp
+
+    name = "linear16_0p5s"
+    V, si, sm, call, expect, meta = load_golden(name)
+    monkeypatch.setattr(bpp, "CAPACITY_PER_WINDOW", 0)
+    monkeypatch.setattr(bpp, "CAPACITY_EXTRA", 8)
+    assert len(expect["event_indices"]) > 8
+    sm2 = copy.deepcopy(sm)
+    got = binary_pursuit(V, np.float32, si, sm2, mode=mode, verbose=False, **call)
+    _assert_same_result(got, expect, name)
+    assert list(sm2["n_spikes"]) == meta["n_spikes_per_unit"]
+
+
 def test_residual_kernel_matches_oracle_order():
     rng = np.random.default_rng(5)
     C, N, M, W = 8, 20000, 5, 61
