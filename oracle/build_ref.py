@@ -19,9 +19,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+# the reference checkout beside the repository, unless FBP_REFERENCE_CL names the kernel file
 REF_CL = os.environ.get(
     "FBP_REFERENCE_CL",
-    "/root/reference/spikesorting_fullpursuit/kernels/binary_pursuit.cl")
+    os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "spikesorting_fullpursuit", "kernels",
+                 "binary_pursuit.cl"))
 LIB = os.path.join(OUT, "libbp_ref.so")
 
 
