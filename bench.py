@@ -47,7 +47,7 @@ METRIC = "binary-pursuit Msample·ch/s, chosen vs plain FP32 on B200, ≥99.9% s
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one
 # launch of the 60 s slice of the linear16 workload, divided by the windows it processed)
 DRAM_PER_UNIT = {
-    "lik_tc_kernel": (17.1e3, "listed", "profiles/lik_tc_kernel_linear16_60s.md: 106.8 MB / 6,240 windows"),
+    "lik_tc_kernel": (17.0e3, "listed", "profiles/lik_tc_persist_kernel_linear16_60s.md: 105.9 MB / 6,240 windows"),
     "partial_corr_kernel": (35.8e3, "flagged", "profiles/partial_corr_kernel_linear16_60s.md: 107.3 MB / 3,001 windows"),
     "screen_kernel": (39.1e3, "flagged", "profiles/screen_kernel_linear16_60s.md: 117.3 MB / 3,001 windows"),
     "argmax_kernel": (25.8e3, "listed", "profiles/argmax_kernel_linear16_60s.md: 160.8 MB / 6,240 windows"),
@@ -346,7 +346,8 @@ def main():
     fma_peak = 148 * 128 * 2 * (clocks.get("sm_mhz") or 1965.0) * 1e6 / 1e12
     fam = {
         "lik_tc_kernel": (st_stage["ms_lik_tc"], "tensor", 2.0 * M * C * W * W * listed,
-                          "2*M*C*W*W flop per listed window (nominal dense product)"),
+                          "2*M*C*W*W flop per listed window (nominal dense product); launched as "
+                          "lik_tc_persist_kernel up to 128 template columns, lik_tc_kernel above"),
         "fixup_kernel": (st_stage["ms_fixup"], "fp32", 2.0 * C * W * 4 * st_stage["fixup_runs_queued"],
                          "2*C*W flop per sample recomputed"),
         "partial_corr_kernel": (st_stage["ms_partial_corr"], "fp32", 2.0 * st_stage["pc_macs"],
