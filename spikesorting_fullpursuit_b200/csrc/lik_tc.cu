@@ -1383,7 +1383,20 @@ bool tc_config(const Dims& d, TcConfig* c)
                             (size_t)kFixCap * 8 + 8 + 4 + (size_t)c->ntiles * 4 + (size_t)c->ntiles * win_slots(d.W) * (16 + d.M) + 8 +
                             1024;
         auto total = [&](uint32_t stages) { return strips + stages * c->group * kstep + (2 + 2 * stages) * 8 + misc; };
-        if (fit < 4 && !tu.lik_stages) {
+        if (c->Np > 128 && !tu.lik_group && !tu.lik_stages) {
+            // above 128 columns (one tile, two CTAs per SM): two stages of as many whole
+            // k-steps as keep both CTAs resident.  Fewer, larger bulk copies and barrier
+            // round trips per MMA; measured on 64 channels x 200 templates: 4 k-steps x 2
+            // stages 249 ms per pursuit's likelihood, against 326 ms for 2 x 3 and 478 ms
+            // for 1 x 7, and 382-513 ms for shapes that leave one CTA per SM
+            const size_t budget = (228 * 1024) / fit - 2 * 1024;
+            c->stages = 2;
+            c->group = 1;
+            while (total(2) <= budget && c->group < 64) {
+                ++c->group;
+                if (total(2) > budget) { --c->group; break; }
+            }
+        } else if (fit < 4 && !tu.lik_stages) {
             // fewer CTAs share the SM: a deeper ring keeps more template bytes in flight
             const size_t budget = (228 * 1024) / fit - 2 * 1024;
             while (c->stages < 8 && total(c->stages + 1) <= budget) ++c->stages;
