@@ -434,10 +434,9 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
         if verbose:
             print("Found a total of ZERO secret spikes", flush=True)
     # side effect of add_n_spikes (neuron_separability.py:334-345)
-    labels_arr = np.asarray(neuron_labels)
-    separability_metrics["n_spikes"] = np.zeros(M)
-    for n in range(M):
-        separability_metrics["n_spikes"][n] = np.count_nonzero(labels_arr == n)
+    labels_arr = np.asarray(neuron_labels, dtype=np.int64)
+    counts = np.bincount(labels_arr, minlength=M)[:M] if labels_arr.size else np.zeros(M, dtype=np.int64)
+    separability_metrics["n_spikes"] = counts.astype(np.float64)
     out = (event_indices, neuron_labels, spike_bool, adjusted_clips)
     if return_stats:
         return out, (pursuer.stats if pursuer else [])
