@@ -925,7 +925,9 @@ int launch_overlap_tables(const Dims& d, const Work& w, const float* T, cudaStre
     const int want_q = (int)tuning().pc_group;
     for (int Q = 8; Q >= 1; Q >>= 1) {
         if (want_q && Q > want_q) continue;
-        const double eff = Q >= 4 ? 1.0 : (Q == 2 ? 1.2 : 1.6);
+        // measured time per unit of work relative to Q = 4: Q = 8 0.72 (64 ch, 200
+        // templates, 60 s) and 0.84 (16 ch, 40 templates, 10 min), Q = 2 1.0-1.2, Q = 1 1.3-1.4
+        const double eff = Q >= 8 ? 0.78 : (Q == 4 ? 1.0 : (Q == 2 ? 1.2 : 1.6));
         uint32_t cu_max = 0;
         double work = 0.0;
         for (uint32_t g0 = 0; g0 < d.M; g0 += Q) {
