@@ -50,7 +50,8 @@ DRAM_PER_UNIT = {
     "lik_tc_kernel": (17.0e3, "listed", "profiles/lik_tc_persist_kernel_linear16_60s.md: 105.9 MB / 6,240 windows"),
     "partial_corr_kernel": (35.8e3, "flagged", "profiles/partial_corr_kernel_linear16_60s.md: 107.3 MB / 3,001 windows"),
     "screen_kernel": (39.1e3, "flagged", "profiles/screen_kernel_linear16_60s.md: 117.3 MB / 3,001 windows"),
-    "argmax_kernel": (25.8e3, "listed", "profiles/argmax_kernel_linear16_60s.md: 160.8 MB / 6,240 windows"),
+    "argmax_kernel": (18.8, "listed", "profiles/residual_accept_compact_linear16_60s.md: argmax_lazy_kernel, "
+                      "0.45 MB / 23,808 windows"),
 }
 
 
@@ -354,7 +355,8 @@ def main():
                                 "2 flop per multiply-add done (device counter)"),
         "screen_kernel": (st_stage["ms_screen"], "latency", None, "L2-latency-bound table scan"),
         "score_kernel": (st_stage["ms_score"], "latency", None, "one sequential C*W chain per candidate"),
-        "argmax_kernel": (st_stage["ms_argmax"], "hbm", 24.0 * listed, "3 window keys (8 B) per listed window"),
+        "argmax_kernel": (st_stage["ms_argmax"], "hbm", 24.0 * listed,
+                          "3 window keys (8 B) per listed window (argmax_lazy_kernel)"),
     }
     kernels = {}
     for name, (ms, bound, work, what) in fam.items():
