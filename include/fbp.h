@@ -275,6 +275,26 @@ int fbp_separability(const void* templates, int templates_f64, const double* cha
                      double* lower_ci, double* threshold, double* contamination, int64_t* peak_channel,
                      void* stream);
 
+/* pairwise_separability (spikesorting_fullpursuit/overlap/neuron_separability.py:348-444,
+ * with optimal_align_templates(align_abs=True, zero_pad=True) of
+ * spikesorting_fullpursuit/overlap/consolidate.py:10-93), all pairs at once.  For each
+ * pair (n1, n2): the shift is the first arg-max over lags [-max_shift, max_shift] of the
+ * absolute cross-correlation of the flattened templates; the templates are aligned per
+ * channel by it and zero padded; pair_matrix[n1][n2] = P(N(E_diff, sd) < 0) with
+ * E_diff = 0.5 SS[n1] - (P1.P2 - 0.5 SS[n2]) and sd^2 the FP64 quadratic form of P1 - P2
+ * with each channel's covariance (0 where that variance is not positive).  Per n1:
+ * noise_misses = P(N(0.5 SS, sd_n1) < threshold), noise_contamination =
+ * P(N(-0.5 SS, sd_n1) > threshold) (NaN where the variance is 0, as scipy gives).
+ * templates [M][C][W] float32 or float64 (templates_f64); template_ss [M] in the same
+ * type; channel_cov float64 [C][W][W]; variance, threshold float64 [M]; pair_matrix
+ * float64 [M][M]; noise_* float64 [M]; optimal_shift int32 [M][M] or NULL.  The
+ * reference uses max_shift = template_len / 4 - 1. */
+int fbp_pair_separability(const void* templates, int templates_f64, const void* template_ss,
+                          const double* channel_cov, const double* variance, const double* threshold,
+                          uint32_t n_templates, uint32_t n_chans, uint32_t template_len, int32_t max_shift,
+                          double* pair_matrix, double* noise_contamination, double* noise_misses,
+                          int32_t* optimal_shift, void* stream);
+
 /* ---- post-pursuit duplicate removal (device-resident output) ---- */
 
 /* Mean clip of one unit, np.mean(clips, axis=0) in float32 (rows summed in

@@ -27,7 +27,8 @@ FBP_TIMING = 0x4
 EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_pursue_chunk", "fbp_pursue_chunk_staged",
            "fbp_adjusted_clips", "fbp_likelihood", "fbp_residual", "fbp_residual_noalloc",
            "fbp_adjoint_loss", "fbp_adjoint_grad", "fbp_mean_clip", "fbp_bp_duplicates_workspace",
-           "fbp_bp_duplicates", "fbp_separability", "fbp_gather_clips", "fbp_robust_template",
+           "fbp_bp_duplicates", "fbp_separability", "fbp_pair_separability", "fbp_gather_clips",
+           "fbp_robust_template",
            "fbp_residual_covariance", "fbp_set_tuning")
 NOALLOC_MAX_SPIKES = 65536
 PASS_RING = 64
@@ -121,6 +122,8 @@ def lib():
     dbl, i32 = ctypes.c_double, ctypes.c_int
     L.fbp_separability.argtypes = [vp, i32, vp, u32, u32, u32, dbl, dbl, i32, vp, vp, vp, vp, vp, vp, vp]
     L.fbp_separability.restype = ctypes.c_int
+    L.fbp_pair_separability.argtypes = [vp, i32, vp, vp, vp, vp, u32, u32, u32, ctypes.c_int32, vp, vp, vp, vp, vp]
+    L.fbp_pair_separability.restype = ctypes.c_int
     L.fbp_gather_clips.argtypes = [vp, u32, ctypes.c_uint64, vp, u32, vp, u32, ctypes.c_int32, u32, vp, vp]
     L.fbp_gather_clips.restype = ctypes.c_int
     L.fbp_robust_template.argtypes = [vp, u32, u32, vp, vp]

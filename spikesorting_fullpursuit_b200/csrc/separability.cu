@@ -130,6 +130,118 @@ __global__ void __launch_bounds__(kSepThreads) separability_kernel(const F* __re
     }
 }
 
+// ---- pairwise_separability (neuron_separability.py:348-444) ----
+//
+// Per pair (n1, n2), one CTA:
+//   shift      first arg-max over lags k in [-max_shift, max_shift] of
+//              |sum_n T1[n+k] T2[n]| over the flattened templates (np.correlate,
+//              mode "full", then its centre slice; consolidate.py:27-41), the sums
+//              in FP64 (float products are exact there)
+//   P1, P2     T1 and T2 aligned per channel by the shift, zero padded
+//              (consolidate.py:43-91): sample i of a channel is kept where
+//              max(shift, 0) <= i < W + min(shift, 0), P1 = T1[i], P2 = T2[i - shift]
+//   var_diff   sum_c (P1 - P2)_c Cov_c (P1 - P2)_c^T     (FP64)
+//   SS12       P1 . P2
+//   E_diff     0.5 SS[n1] - (SS12 - 0.5 SS[n2])
+//   pair       var_diff > 0 ? P(N(E_diff, sqrt(var_diff)) < 0) : 0
+// The reference keeps its types: with shift 0 it works on the templates
+// themselves (their own type: the difference, the dot product and E_diff are
+// float32 for float32 templates), otherwise on float64 zero-padded copies.
+// Float32 dot products here are the FP64 sum rounded once (the reference's
+// BLAS order is not specified); FP64 sums agree to rounding.
+constexpr int kPairThreads = 256;
+
+__device__ __forceinline__ double ndtr_upper(double x)   // P(Z > x) = 0.5 erfc(x / sqrt 2)
+{
+    return 0.5 * erfc(x * 0.70710678118654752440);
+}
+
+template <class F>
+__global__ void __launch_bounds__(kPairThreads) pair_separability_kernel(
+    const F* __restrict__ T, const F* __restrict__ ss, const double* __restrict__ cov,
+    const double* __restrict__ variance, const double* __restrict__ threshold, uint32_t M, uint32_t C, uint32_t W,
+    int max_shift, double* pair, double* noise_contamination, double* noise_misses, int32_t* shift_out)
+{
+    typedef cub::BlockReduce<double, kPairThreads> RD;
+    __shared__ typename RD::TempStorage rd;
+    __shared__ int s_shift;
+    extern __shared__ __align__(16) unsigned char sraw[];
+    const uint32_t n1 = blockIdx.y, n2 = blockIdx.x;
+    const uint32_t L = C * W, nlag = 2u * (uint32_t)max_shift + 1u;
+    F* t1 = reinterpret_cast<F*>(sraw);
+    F* t2 = t1 + L;
+    double* cc = reinterpret_cast<double*>(sraw + (((size_t)2 * L * sizeof(F) + 15) & ~(size_t)15));   // [nlag]
+    for (uint32_t e = threadIdx.x; e < L; e += blockDim.x) {
+        t1[e] = T[(uint64_t)n1 * L + e];
+        t2[e] = T[(uint64_t)n2 * L + e];
+    }
+    __syncthreads();
+    // |cross-correlation| at each lag of the centre slice, one warp per lag
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (uint32_t li = warp; li < nlag; li += nwarps) {
+        const int k = (int)li - max_shift;
+        const uint32_t lo = k < 0 ? (uint32_t)(-k) : 0u, hi = k > 0 ? L - (uint32_t)k : L;
+        double acc = 0.0;
+        for (uint32_t n = lo + lane; n < hi; n += 32) acc = fma((double)t1[n + k], (double)t2[n], acc);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) cc[li] = fabs(acc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t best = 0;
+        for (uint32_t li = 1; li < nlag; ++li)
+            if (cc[li] > cc[best]) best = li;   // first maximum
+        s_shift = (int)best - max_shift;
+    }
+    __syncthreads();
+    const int sh = s_shift;
+    const bool same_type = sh == 0;   // the reference works on the templates themselves
+    const int ilo = sh > 0 ? sh : 0, ihi = (int)W + (sh < 0 ? sh : 0);
+    // aligned difference of channel c at sample i, in the type the reference forms it in
+    auto diff = [&](uint32_t c, int i) -> double {
+        if (i < ilo || i >= ihi) return 0.0;
+        const F a = t1[c * W + i], b = t2[(int)(c * W) + i - sh];
+        return same_type ? (double)(F)(a - b) : (double)a - (double)b;
+    };
+    double qpart = 0.0, dpart = 0.0;
+    for (uint32_t e = threadIdx.x; e < L; e += blockDim.x) {
+        const uint32_t c = e / W;
+        const int i = (int)(e - c * W);
+        const double di = diff(c, i);
+        if (i >= ilo && i < ihi) dpart = fma((double)t1[e], (double)t2[(int)e - sh], dpart);
+        if (di == 0.0) continue;
+        const double* row = cov + ((uint64_t)c * W + (uint32_t)i) * W;
+        double r = 0.0;
+        for (int j = ilo; j < ihi; ++j) r = fma(row[j], diff(c, j), r);
+        qpart = fma(di, r, qpart);
+    }
+    const double var_diff = RD(rd).Sum(qpart);
+    __syncthreads();
+    const double ss12 = RD(rd).Sum(dpart);
+    if (threadIdx.x == 0) {
+        const F e1 = (F)0.5 * ss[n1];   // expected n1 likelihood given an n1 spike
+        double e_diff;
+        if (same_type) {
+            const F e2 = (F)ss12 - (F)0.5 * ss[n2];
+            e_diff = (double)(F)(e1 - e2);
+        } else {
+            const double e2 = ss12 - (double)((F)0.5 * ss[n2]);
+            e_diff = (double)e1 - e2;
+        }
+        // norm.cdf(0, E_diff, sd) = P(Z > E_diff / sd)
+        pair[(uint64_t)n1 * M + n2] = var_diff > 0.0 ? ndtr_upper(e_diff / sqrt(var_diff)) : 0.0;
+        if (shift_out) shift_out[(uint64_t)n1 * M + n2] = sh;
+        if (n2 == 0) {
+            const double sd = sqrt(variance[n1]), thr = threshold[n1], e = (double)e1;
+            const double nan = __longlong_as_double(0x7ff8000000000000ll);
+            // norm.cdf(thr, E, sd) and norm.sf(thr, -E, sd); scipy gives NaN for sd == 0
+            noise_misses[n1] = sd > 0.0 ? ndtr_upper((e - thr) / sd) : nan;
+            noise_contamination[n1] = sd > 0.0 ? ndtr_upper((thr + e) / sd) : nan;
+        }
+    }
+}
+
 }  // namespace
 }  // namespace fbp
 
@@ -158,6 +270,47 @@ extern "C" int fbp_separability(const void* templates, int templates_f64, const 
         separability_kernel<float><<<n_templates, kSepThreads, 0, st>>>(
             static_cast<const float*>(templates), channel_cov, n_chans, template_len, sigma_bp_noise, sigma_bp_ci,
             apply_bp_threshold, out);
+    FBP_CUDA(cudaGetLastError());
+    return FBP_OK;
+}
+
+extern "C" int fbp_pair_separability(const void* templates, int templates_f64, const void* template_ss,
+                                     const double* channel_cov, const double* variance, const double* threshold,
+                                     uint32_t n_templates, uint32_t n_chans, uint32_t template_len, int32_t max_shift,
+                                     double* pair_matrix, double* noise_contamination, double* noise_misses,
+                                     int32_t* optimal_shift, void* stream)
+{
+    set_error("");
+    if (n_templates == 0) return FBP_OK;
+    if (n_chans == 0 || template_len == 0) return fail(FBP_E_ARG, "invalid sizes");
+    if (max_shift < 0 || (uint32_t)max_shift >= template_len)
+        return fail(FBP_E_ARG, "max_shift must lie in [0, template_len)");
+    if (n_templates > 65535) return fail(FBP_E_ARG, "at most 65535 templates");
+    if (!templates || !template_ss || !channel_cov || !variance || !threshold || !pair_matrix ||
+        !noise_contamination || !noise_misses)
+        return fail(FBP_E_ARG, "null pointer argument");
+    const uint64_t L = (uint64_t)n_chans * template_len;
+    const size_t fsz = templates_f64 ? 8 : 4;
+    const size_t smem = ((2 * L * fsz + 15) & ~(size_t)15) + (size_t)(2 * max_shift + 1) * 8;
+    int dev = 0, optin = 0;
+    FBP_CUDA(cudaGetDevice(&dev));
+    FBP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (L >= (1ull << 31) || smem + 2048 > (size_t)optin) return fail(FBP_E_ARG, "templates too long for one CTA");
+    const dim3 grid(n_templates, n_templates);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (templates_f64) {
+        FBP_CUDA(allow_max_dyn_smem(pair_separability_kernel<double>));
+        pair_separability_kernel<double><<<grid, kPairThreads, smem, st>>>(
+            static_cast<const double*>(templates), static_cast<const double*>(template_ss), channel_cov, variance,
+            threshold, n_templates, n_chans, template_len, max_shift, pair_matrix, noise_contamination, noise_misses,
+            optimal_shift);
+    } else {
+        FBP_CUDA(allow_max_dyn_smem(pair_separability_kernel<float>));
+        pair_separability_kernel<float><<<grid, kPairThreads, smem, st>>>(
+            static_cast<const float*>(templates), static_cast<const float*>(template_ss), channel_cov, variance,
+            threshold, n_templates, n_chans, template_len, max_shift, pair_matrix, noise_contamination, noise_misses,
+            optimal_shift);
+    }
     FBP_CUDA(cudaGetLastError());
     return FBP_OK;
 }

@@ -10,6 +10,14 @@ thresholds, tail probabilities, peak channels) runs in libfbp.so
 (csrc/separability.cu).  Template energies, expectations, peak channels are
 bit-identical to the reference; variances and the values derived from them
 agree to FP64 rounding (the reference sums its matrix products with BLAS).
+
+``pairwise_separability`` (neuron_separability.py:348-444) estimates, for every
+pair of units, the probability that a spike of one is taken for the other, and
+per unit the probabilities of missing a spike or adding noise.  Each pair's
+templates are aligned by the arg-max of their absolute cross-correlation
+(consolidate.optimal_align_templates with align_abs=True, zero_pad=True) and
+compared through the FP64 quadratic form of their difference with the channel
+covariances; all pairs run at once on the device (csrc/separability.cu).
 """
 from __future__ import annotations
 
@@ -100,3 +108,52 @@ def bp_thresholds(templates, channel_covariance_mats, n_chans, W, sigma_bp_noise
     _, ss, _, _, thr, _, _ = _device_metrics(np.vstack(templates), channel_covariance_mats, n_chans, W,
                                              sigma_bp_noise, sigma_bp_CI, True, device)
     return ss, thr
+
+
+def _pair_metrics(separability_metrics, sort_info, device=None):
+    """(pair matrix, noise contamination, noise misses, optimal shifts) of all pairs."""
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("No GPU available")
+    dev = (device if isinstance(device, torch.device)
+           else torch.device("cuda", torch.cuda.current_device() if device is None else int(device)))
+    n_chans = sort_info["n_channels"]
+    W = int(separability_metrics["bp_n_samples_per_chan"])
+    max_shift = (W // 4) - 1
+    T = np.ascontiguousarray(separability_metrics["templates"])
+    if T.dtype not in (np.float32, np.float64):
+        T = T.astype(np.float64)
+    M = T.shape[0]
+    if max_shift < 0:
+        # the reference's arg-max over an empty lag range
+        raise ValueError("attempt to get argmax of an empty sequence")
+    if M == 0:
+        return np.zeros((0, 0)), np.zeros(0), np.zeros(0), np.zeros((0, 0), dtype=np.int32)
+    ss = np.ascontiguousarray(np.asarray(separability_metrics["template_SS"]).astype(T.dtype, copy=False))
+    covs = separability_metrics["channel_covariance_mats"]
+    cov = np.ascontiguousarray(np.stack([np.asarray(c, dtype=np.float64).reshape(W, W) for c in covs[:n_chans]]))
+    var = np.ascontiguousarray(np.asarray(separability_metrics["neuron_variances"], dtype=np.float64))
+    thr = np.ascontiguousarray(np.asarray(separability_metrics["neuron_lower_thresholds"], dtype=np.float64))
+    Td = torch.from_numpy(T.reshape(M, n_chans * W)).to(dev)
+    ssd, covd, vard, thrd = (torch.from_numpy(a).to(dev) for a in (ss, cov, var, thr))
+    pair = torch.empty((M, M), dtype=torch.float64, device=dev)
+    contamination = torch.empty(M, dtype=torch.float64, device=dev)
+    misses = torch.empty(M, dtype=torch.float64, device=dev)
+    shifts = torch.empty((M, M), dtype=torch.int32, device=dev)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    _native.check(_native.lib().fbp_pair_separability(
+        _ptr(Td), int(T.dtype == np.float64), _ptr(ssd), _ptr(covd), _ptr(vard), _ptr(thrd), M, n_chans, W,
+        max_shift, _ptr(pair), _ptr(contamination), _ptr(misses), _ptr(shifts), stream))
+    return pair.cpu().numpy(), contamination.cpu().numpy(), misses.cpu().numpy(), shifts.cpu().numpy()
+
+
+def pairwise_separability(separability_metrics, sort_info, device=None):
+    """neuron_separability.pairwise_separability on the GPU: returns
+    (pair_separability_matrix, noise_contamination, noise_misses).
+    pair_separability_matrix[n1, n2] is the probability that the likelihood of
+    unit n2 exceeds that of unit n1 given an n1 spike; noise_misses[n] the
+    probability that a spike of n stays below its threshold; noise_contamination[n]
+    the probability that noise alone crosses it."""
+    pair, contamination, misses, _ = _pair_metrics(separability_metrics, sort_info, device)
+    return pair, contamination, misses
