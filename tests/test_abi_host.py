@@ -157,3 +157,25 @@ def test_tuning_validation(lib):
     t = _native.FbpTuning(1, 2, 4, 4, 3)
     assert lib.fbp_set_tuning(ctypes.byref(t)) == _native.FBP_OK
     assert lib.fbp_set_tuning(None) == _native.FBP_OK
+
+
+def test_pair_separability_arguments_fail_before_any_device_call(lib):
+    fake = ctypes.c_void_p(16)   # never dereferenced: validation rejects the call first
+
+    def call(M=4, C=4, W=40, max_shift=9, ptrs=(fake,) * 9):
+        t, ss, cov, var, thr, pair, cont, miss, sh = ptrs
+        return lib.fbp_pair_separability(t, 0, ss, cov, var, thr, M, C, W, max_shift, pair, cont, miss, sh, None)
+
+    # no templates: nothing to do
+    assert call(M=0) == _native.FBP_OK
+    for kw, msg in (({"C": 0}, b"invalid sizes"), ({"W": 0}, b"invalid sizes"),
+                    ({"max_shift": -1}, b"max_shift"), ({"max_shift": 40}, b"max_shift"),
+                    ({"M": 65536}, b"65535")):
+        assert call(**kw) == _native.FBP_E_ARG, kw
+        assert msg in lib.fbp_last_error(), kw
+    # every input and the three result arrays are required; the shift matrix is optional
+    for k in range(8):
+        ptrs = [fake] * 9
+        ptrs[k] = None
+        assert call(ptrs=tuple(ptrs)) == _native.FBP_E_ARG, k
+        assert b"null" in lib.fbp_last_error(), k
