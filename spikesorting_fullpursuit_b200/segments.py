@@ -101,7 +101,10 @@ def pursue_segments(segments, pursue: Callable = None, group=None, streams: int 
     sequential run would not chunk it (chunk boundaries, and the duplicates the
     reference leaves in chunk overlaps, follow the budget).
     Returns the list of results in segment order on every rank.  Without an
-    initialised process group everything runs locally."""
+    initialised process group everything runs locally.  A rank whose pursuit
+    fails still takes part in the final gather, so no rank waits on it: the
+    failing rank re-raises its own error, the others raise RuntimeError naming
+    the lowest failing rank."""
     import torch.distributed as dist
 
     default = pursue is None
@@ -112,12 +115,23 @@ def pursue_segments(segments, pursue: Callable = None, group=None, streams: int 
     rank = dist.get_rank(group) if dist_on else 0
     lengths = [int(seg[0].shape[1]) for seg in segments]
     mine = shard_segments(lengths, world)[rank]
-    local = _run_local(segments, mine, lengths, pursue, int(streams), kwargs, default)
     if not dist_on:
+        local = _run_local(segments, mine, lengths, pursue, int(streams), kwargs, default)
         return [local[i] for i in range(len(segments))]
+    error = None
+    try:
+        local = _run_local(segments, mine, lengths, pursue, int(streams), kwargs, default)
+    except Exception as exc:   # every rank must still reach the gather below
+        local, error = {}, exc
     gathered = [None] * world
-    dist.all_gather_object(gathered, local, group=group)
+    dist.all_gather_object(gathered, (local, None if error is None else "%s: %s" % (type(error).__name__, error)),
+                           group=group)
+    if error is not None:
+        raise error
+    failed = [(r, msg) for r, (_, msg) in enumerate(gathered) if msg is not None]
+    if failed:
+        raise RuntimeError("segment pursuit failed on rank %d: %s" % failed[0])
     out = {}
-    for part in gathered:
+    for part, _ in gathered:
         out.update(part)
     return [out[i] for i in range(len(segments))]

@@ -65,6 +65,43 @@ def test_two_ranks_gather_every_segment_in_order():
         assert out[1] == want
 
 
+def _pursue_failing_on_segment_2(voltage, tag):
+    if tag == 2:
+        raise ValueError("bad segment %d" % tag)
+    return _fake_pursue(voltage, tag)
+
+
+def _failing_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    # a short timeout: a rank left waiting in the gather would fail this test, not hang it
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=30))
+    try:
+        pursue_segments(_segments(), pursue=_pursue_failing_on_segment_2)
+        out[rank] = "returned"
+    except Exception as exc:
+        out[rank] = "%s: %s" % (type(exc).__name__, exc)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_a_failing_rank_does_not_leave_the_others_waiting():
+    owner = next(r for r, sh in enumerate(shard_segments([s[0].shape[1] for s in _segments()], 2)) if 2 in sh)
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        assert out[owner] == "ValueError: bad segment 2"
+        assert out[1 - owner] == "RuntimeError: segment pursuit failed on rank %d: ValueError: bad segment 2" % owner
+
+
 def test_without_process_group_runs_locally():
     res = pursue_segments(_segments(), pursue=_fake_pursue)
     assert len(res) == 5 and all(r[1][0] == k for k, r in enumerate(res) if r[1].size)
