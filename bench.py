@@ -267,7 +267,7 @@ def main():
             ev0.record(stream)
             _native.check(lib.fbp_pursue_chunk(ctypes.byref(d), flags, P(Vw), P(Td), P(bd), P(thd), P(ws),
                                                ws.numel(), P(idx), P(lab), cap, ctypes.byref(n),
-                                               ctypes.byref(st), 0, sptr))
+                                               ctypes.byref(st), _native.MAX_PASSES, sptr))
             ev1.record(stream)
             torch.cuda.synchronize()
             if i >= warmup:
@@ -533,7 +533,7 @@ def run_batched(args):
         n = ctypes.c_uint32(0)
         _native.check(lib.fbp_pursue_chunk(ctypes.byref(j["d"]), flags, P(j["V"]), P(j["T"]), P(j["b"]), P(j["th"]),
                                            P(j["ws"]), j["ws"].numel(), P(j["idx"]), P(j["lab"]), j["cap"],
-                                           ctypes.byref(n), None, 0, ctypes.c_void_p(stream.cuda_stream)))
+                                           ctypes.byref(n), None, _native.MAX_PASSES, ctypes.c_void_p(stream.cuda_stream)))
         j["n"] = n.value
 
     def step(nstreams):

@@ -31,6 +31,7 @@ EXPORTS = ("fbp_abi_version", "fbp_last_error", "fbp_workspace_bytes", "fbp_purs
            "fbp_robust_template",
            "fbp_residual_covariance", "fbp_set_tuning")
 NOALLOC_MAX_SPIKES = 65536
+MAX_PASSES = 2048   # default pass limit of one chunk (the reference's loop has none)
 PASS_RING = 64
 ABI_VERSION = 4
 

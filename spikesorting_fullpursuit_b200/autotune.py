@@ -143,7 +143,7 @@ def tune(voltage, templates, bias, theta, W, S, overlap=True, sample_s=None, sam
         st = _native.FbpChunkStats()
         _native.check(L.fbp_pursue_chunk(ctypes.byref(d), flags | (_native.FBP_TIMING if timing else 0), _ptr(Vw),
                                          _ptr(T), _ptr(b), _ptr(th), _ptr(ws), ws.numel(), _ptr(idx), _ptr(lab), cap,
-                                         ctypes.byref(k), ctypes.byref(st), 0, stream))
+                                         ctypes.byref(k), ctypes.byref(st), _native.MAX_PASSES, stream))
         return st
 
     best, best_ms = None, None

@@ -50,7 +50,7 @@ from .. import _native, autotune
 from ..processing.conversions import time_window_to_samples
 
 WORK_GROUP_SIZE = 256
-MAX_PASSES = 2048          # default pass limit of one chunk
+MAX_PASSES = _native.MAX_PASSES   # default pass limit of one chunk
 MAX_CAPACITY_RETRIES = 4   # re-runs of a chunk whose spikes outgrew the output buffers
 CAPACITY_PER_WINDOW = 16   # spike slots of a chunk's first attempt, per window ...
 CAPACITY_EXTRA = 1024      # ... plus these
