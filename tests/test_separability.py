@@ -4,7 +4,6 @@ Template energies, peak channels and per-channel noise fractions are
 bit-exact; variances and what derives from them agree to FP64 rounding
 (rtol 1e-12; tail probabilities 1e-9), since the reference's matrix products
 run in BLAS order."""
-import copy
 import importlib.util
 import os
 
