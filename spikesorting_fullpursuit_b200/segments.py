@@ -32,6 +32,15 @@ def shard_segments(lengths: Sequence[int], world_size: int) -> List[List[int]]:
     return shards
 
 
+def worker_budget(total_memory, streams, n_segments):
+    """Device bytes each of ``min(streams, n_segments)`` concurrent pursuits
+    plans its chunks for: an equal share of the budget the reference gives one
+    pursuit, max(total / 2, total - 1 GiB) (binary_pursuit_parallel.py:389-408),
+    so the workers together stay within it."""
+    budget = max(0.5 * total_memory, total_memory - (1 << 30))
+    return budget / max(1, min(int(streams), int(n_segments)))
+
+
 def _run_local(segments, mine, lengths, pursue, streams, kwargs, pursue_is_default=False):
     """Results of this rank's segments, by segment index.  With streams > 1 the
     segments (longest first) are taken by that many worker threads; on a CUDA
@@ -48,12 +57,8 @@ def _run_local(segments, mine, lengths, pursue, streams, kwargs, pursue_is_defau
     use_cuda = torch.cuda.is_available()
     device = torch.cuda.current_device() if use_cuda else None
     if use_cuda and pursue_is_default and kwargs.get("max_gpu_memory") is None:
-        # each concurrent pursuit plans its chunks for a share of the device budget
-        # the reference uses for one (binary_pursuit_parallel.py:389-408), so the
-        # workers together stay within it
         total = torch.cuda.get_device_properties(device).total_memory
-        budget = max(0.5 * total, total - (1 << 30))
-        kwargs = dict(kwargs, max_gpu_memory=budget / min(streams, len(mine)))
+        kwargs = dict(kwargs, max_gpu_memory=worker_budget(total, streams, len(mine)))
     todo = queue.Queue()
     for i in sorted(mine, key=lambda k: (-lengths[k], k)):
         todo.put(i)

@@ -6,7 +6,8 @@ import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
-from spikesorting_fullpursuit_b200.segments import pursue_segments, shard_segments
+from spikesorting_fullpursuit_b200.overlap.binary_pursuit_parallel import plan_chunks
+from spikesorting_fullpursuit_b200.segments import pursue_segments, shard_segments, worker_budget
 
 
 def test_shards_are_balanced_and_deterministic():
@@ -124,3 +125,19 @@ def test_concurrent_workers_reraise_the_first_failing_segment():
 
     with pytest.raises(RuntimeError, match="segment 1"):
         pursue_segments(_segments(), pursue=pursue, streams=4)
+
+
+def test_concurrent_pursuits_share_one_pursuit_budget():
+    gib = 1 << 30
+    total = 183 * gib
+    one = total - gib   # the reference's budget for one pursuit on a 183 GiB device
+    assert worker_budget(total, 1, 5) == one
+    assert worker_budget(total, 4, 5) * 4 == one
+    assert worker_budget(total, 8, 3) * 3 == one   # no more workers than segments
+    assert worker_budget(2 * gib, 2, 2) == gib / 2  # small devices keep half for one pursuit
+    # chunks planned for a worker's share fit that share: a 30 min 64-channel segment that is
+    # one chunk alone is cut into several when eight run at once
+    args = (1800 * 30000, 64, 200, 76, 30000, 75, total)
+    on1, chunk1 = plan_chunks(*args, max_gpu_memory=worker_budget(total, 1, 8))
+    on8, chunk8 = plan_chunks(*args, max_gpu_memory=worker_budget(total, 8, 8))
+    assert len(on1) == 1 and len(on8) > 1 and chunk8 < chunk1
