@@ -179,3 +179,30 @@ def test_pair_separability_arguments_fail_before_any_device_call(lib):
         ptrs[k] = None
         assert call(ptrs=tuple(ptrs)) == _native.FBP_E_ARG, k
         assert b"null" in lib.fbp_last_error(), k
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the behaviour without a GPU")
+def test_public_functions_fail_loudly_without_a_gpu():
+    """No CPU fallback: every GPU-backed drop-in raises the reference's own error
+    (binary_pursuit_parallel.py:292-293) when no CUDA device is present."""
+    from spikesorting_fullpursuit_b200 import binary_pursuit, postprocessing, synth
+    from spikesorting_fullpursuit_b200.overlap import full_binary_pursuit, neuron_separability
+    from spikesorting_fullpursuit_b200.processing import clip_utils
+
+    V, si, sm, _ = synth.make_recording(3, n_chans=2, duration_s=0.05, n_units=2, n_cov_clips=100)
+    W = si["n_samples_per_chan"]
+    covs = [np.eye(W) for _ in range(2)]
+    sm_cov = dict(sm, channel_covariance_mats=covs)
+    calls = [
+        lambda: binary_pursuit(V, np.float32, si, sm),
+        lambda: neuron_separability.compute_separability_metrics(list(sm["templates"]), covs, si),
+        lambda: neuron_separability.pairwise_separability(sm_cov, si),
+        lambda: clip_utils.get_clips({"sampling_rate": si["sampling_rate"]}, V, [0], np.array([100]), si["clip_width"]),
+        lambda: clip_utils.calculate_robust_template(np.zeros((3, W), dtype=np.float32)),
+        lambda: postprocessing.remove_binary_pursuit_duplicates(np.array([5, 7]), np.zeros((2, W), np.float32),
+                                                                np.zeros(W, np.float32), np.ones(2, bool), 3),
+        lambda: full_binary_pursuit.get_channel_covariance_matrix(np.zeros((4, 2 * W), np.float32), 2, W, 4, False),
+    ]
+    for call in calls:
+        with pytest.raises(RuntimeError, match="No GPU available"):
+            call()
