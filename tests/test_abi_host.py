@@ -206,3 +206,45 @@ def test_public_functions_fail_loudly_without_a_gpu():
     for call in calls:
         with pytest.raises(RuntimeError, match="No GPU available"):
             call()
+
+
+C_CONSUMER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "fbp.h"
+
+int main(void)
+{
+    fbp_dims d = {16, 400000, 40, 101, 100, 256};
+    fbp_dims bad = {0, 1000, 4, 101, 100, 256};
+    uint32_t n = 0;
+    int rc;
+    if (fbp_abi_version() != FBP_ABI_VERSION) return 1;
+    if (fbp_workspace_bytes(&d, FBP_OVERLAP_RECHECK) <= fbp_workspace_bytes(&d, FBP_PLAIN_FP32)) return 2;
+    if (fbp_workspace_bytes(&bad, 0) != 0) return 3;
+    rc = fbp_pursue_chunk(&bad, 0, NULL, NULL, NULL, NULL, NULL, 0, NULL, NULL, 0, &n, NULL, 2048, NULL);
+    if (rc != FBP_E_ARG || strlen(fbp_last_error()) == 0) return 4;
+    printf("ok %d\n", fbp_abi_version());
+    return 0;
+}
+"""
+
+
+def test_header_compiles_as_c_and_links_the_library(lib, tmp_path):
+    """A C99 program that includes include/fbp.h and links libfbp.so runs the host-side
+    paths of the ABI (version, workspace sizes, argument rejection) without a GPU."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "consumer.c"
+    src.write_text(C_CONSUMER)
+    exe = tmp_path / "consumer"
+    libdir = os.path.dirname(build.LIB)
+    subprocess.check_call([gcc, "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", os.path.join(REPO, "include"),
+                           str(src), "-o", str(exe), "-L", libdir, "-l:libfbp.so", "-Wl,-rpath," + libdir])
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, (out.returncode, out.stderr)
+    assert out.stdout.strip() == "ok %d" % _native.ABI_VERSION
