@@ -886,6 +886,9 @@ struct PcConfig {
     size_t smem = 0;
 };
 
+// The partial-correlation launch shape of the calling thread's current chunk:
+// launch_overlap_tables sets it and launch_overlap_fast reads it, both inside the
+// same fbp_pursue_chunk call on that thread, so no other call can come between them.
 PcConfig& pc_config()
 {
     static thread_local PcConfig c;
